@@ -1,0 +1,202 @@
+"""B200-native GustANN all-in-GPU search path.
+
+Python mirror of the reference's host interface (``gustann::GustANN``,
+src/ssd_search.hpp:18-83) over the C ABI of ``libgann.so`` (include/gann.h):
+
+    g = GustANN(DataType.UINT8)
+    g.init_pure_mem(GustANNConfig(index_file, pq_file_prefix, nav_graph_prefix), use_gpu_mem=True)
+    g.search(qdata, num_queries, topk, ef_search, nns, distances, found_cnt, stats)
+
+Errors are raised as :class:`GustANNError` carrying the ABI status code (the
+reference aborts, exits or throws instead). The search runs only through the
+CUDA library; there is no CPU fallback, and importing fails loudly when the
+library has not been built.
+"""
+from __future__ import annotations
+
+import ctypes
+import enum
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+
+_LIB_PATH = Path(__file__).resolve().parent / "libgann.so"
+_lib = None
+
+GANN_OK, GANN_EINVAL, GANN_EIO, GANN_EFORMAT, GANN_ECUDA, GANN_ENOMEM, GANN_EKERNEL, GANN_ERANGE = range(8)
+PREC_FP32, PREC_BF16, PREC_BF16X3 = 0, 1, 2
+
+
+class DataType(enum.IntEnum):
+    """gustann::DataType, src/common.hpp:22-25."""
+
+    UINT8 = 0
+    FLOAT = 1
+
+
+@dataclass
+class GustANNConfig:
+    """gustann::GustANNConfig, src/ssd_search.hpp:18-23."""
+
+    index_file: str = ""
+    pq_file_prefix: str = ""
+    nav_graph_prefix: str = ""
+
+
+@dataclass
+class GustANNStats:
+    """gustann::GustANNStats, src/ssd_search.hpp:25-27 (seconds)."""
+
+    run_time: float = 0.0
+
+
+class GustANNError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[gann status {code}] {msg}")
+        self.code = code
+
+
+class GannInfo(ctypes.Structure):
+    _fields_ = [
+        ("num_points", ctypes.c_int64), ("dim", ctypes.c_int64), ("max_degree", ctypes.c_int64),
+        ("medoid", ctypes.c_int64), ("node_len", ctypes.c_int64), ("nodes_per_page", ctypes.c_int64),
+        ("num_pages", ctypes.c_int64), ("pq_chunks", ctypes.c_int32), ("dtype", ctypes.c_int32),
+        ("has_nav", ctypes.c_int32), ("nav_points", ctypes.c_int32), ("nav_max_degree", ctypes.c_int32),
+        ("device", ctypes.c_int32), ("device_bytes", ctypes.c_int64),
+    ]
+
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_SIGNATURES = {
+    "gann_open": (_I, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, _I, _I, ctypes.POINTER(_P)]),
+    "gann_close": (_I, [_P]),
+    "gann_get_info": (_I, [_P, ctypes.POINTER(GannInfo)]),
+    "gann_search": (_I, [_P, _P, _I, _I, _I, _P, _P, _P, ctypes.POINTER(ctypes.c_double)]),
+    "gann_search_device": (_I, [_P, _P, _I, _I, _I, _P, _P, _P, _P]),
+    "gann_check": (_I, [_P, _P]),
+    "gann_set_fma": (_I, [_P, _I, _I]),
+    "gann_last_error": (ctypes.c_char_p, []),
+    "gann_sample_pivots": (_I, [ctypes.c_int64, ctypes.c_int64, ctypes.c_uint32, _P]),
+}
+
+
+def lib() -> ctypes.CDLL:
+    """Load libgann.so (built in-tree by gustann_b200/build.py)."""
+    global _lib
+    if _lib is None:
+        if not _LIB_PATH.exists():
+            raise ImportError(f"{_LIB_PATH} is missing: run `python gustann_b200/build.py` "
+                              "(the search path has no CPU fallback)")
+        L = ctypes.CDLL(str(_LIB_PATH))
+        for name, (res, args) in _SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def exported_symbols() -> list[str]:
+    return list(_SIGNATURES)
+
+
+def _check(rc: int) -> None:
+    if rc != GANN_OK:
+        msg = lib().gann_last_error()
+        raise GustANNError(rc, msg.decode() if msg else "")
+
+
+def _ptr(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+def sample_pivots(num_data: int, num_samp: int, seed: int = 114514) -> np.ndarray:
+    """The pivot-graph sample of bin/gen_small_file.cpp:12-25 (sorted global ids)."""
+    out = np.empty(num_samp, dtype=np.int32)
+    _check(lib().gann_sample_pivots(num_data, num_samp, seed, _ptr(out)))
+    return out
+
+
+class GustANN:
+    """gustann::GustANN (src/ssd_search.hpp:29-83), all-in-GPU mode."""
+
+    def __init__(self, data_type: DataType = DataType.FLOAT):
+        self.data_type = DataType(data_type)
+        self._h = None
+
+    def init_pure_mem(self, config: GustANNConfig, use_gpu_mem: bool = True, validate: bool = True) -> None:
+        """GustANN::init_pure_mem (src/ssd_search.cu:108-112). Only the HBM-resident
+        mode (``-G``) is provided; ``use_gpu_mem=False`` (records in host DRAM) is refused."""
+        if not use_gpu_mem:
+            raise GustANNError(GANN_EINVAL, "records in host memory (use_gpu_mem=False) are not provided")
+        if self._h is not None:
+            self.close()
+        h = _P()
+        nav = config.nav_graph_prefix.encode() if config.nav_graph_prefix else None
+        _check(lib().gann_open(config.index_file.encode(), config.pq_file_prefix.encode(), nav,
+                               int(self.data_type), 0 if validate else 1, ctypes.byref(h)))
+        self._h = h
+
+    @property
+    def handle(self):
+        if self._h is None:
+            raise GustANNError(GANN_EINVAL, "not initialised: call init_pure_mem first")
+        return self._h
+
+    def info(self) -> dict:
+        inf = GannInfo()
+        _check(lib().gann_get_info(self.handle, ctypes.byref(inf)))
+        return {f: getattr(inf, f) for f, _ in GannInfo._fields_}
+
+    def set_fma(self, table: bool, exact: bool) -> None:
+        _check(lib().gann_set_fma(self.handle, int(table), int(exact)))
+
+    def search(self, qdata: np.ndarray, num_queries: int, topk: int, ef_search: int, nns: np.ndarray,
+               distances: np.ndarray, found_cnt: np.ndarray, stats: GustANNStats | None = None) -> None:
+        """GustANN::search (src/ssd_search.hpp:78-80): fills nns (nq x topk int32),
+        distances (nq x topk float32, squared L2) and found_cnt (nq int32)."""
+        q = np.ascontiguousarray(qdata, dtype=np.float32)
+        for a, dt in ((nns, np.int32), (distances, np.float32), (found_cnt, np.int32)):
+            if a.dtype != dt or not a.flags.c_contiguous:
+                raise GustANNError(GANN_EINVAL, "output buffers must be C-contiguous int32/float32/int32")
+        if q.size < num_queries * self.info()["dim"] or nns.size < num_queries * topk or \
+                distances.size < num_queries * topk or found_cnt.size < num_queries:
+            raise GustANNError(GANN_EINVAL, "buffer smaller than num_queries requires")
+        t = ctypes.c_double(0.0)
+        _check(lib().gann_search(self.handle, _ptr(q), int(num_queries), int(topk), int(ef_search),
+                                 _ptr(nns), _ptr(distances), _ptr(found_cnt), ctypes.byref(t)))
+        if stats is not None:
+            stats.run_time = t.value
+
+    def query(self, q: np.ndarray, topk: int, ef_search: int):
+        """Convenience form of :meth:`search` returning (ids, distances, found, seconds)."""
+        q = np.ascontiguousarray(q, dtype=np.float32)
+        nq = q.shape[0]
+        nns = np.zeros((nq, topk), np.int32)
+        dis = np.zeros((nq, topk), np.float32)
+        fnd = np.zeros(nq, np.int32)
+        st = GustANNStats()
+        self.search(q, nq, topk, ef_search, nns, dis, fnd, st)
+        return nns, dis, fnd, st.run_time
+
+    def search_device(self, d_q: int, nq: int, topk: int, ef_search: int, d_nns: int, d_dists: int,
+                      d_found: int, stream: int = 0) -> None:
+        """Device-pointer form (gann_search_device); enqueued without a host sync."""
+        _check(lib().gann_search_device(self.handle, d_q, nq, topk, ef_search, d_nns, d_dists, d_found,
+                                        stream or None))
+
+    def check(self, stream: int = 0) -> None:
+        _check(lib().gann_check(self.handle, stream or None))
+
+    def close(self) -> None:
+        if self._h is not None:
+            lib().gann_close(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,383 @@
+// C ABI of libgann: index loading into HBM and the search entry points.
+//
+// gann_open   ~ GustANN::GustANN + GustANN::init_pure_mem(cfg, true)  (src/ssd_search.cu:55-112,
+//               src/pure_mem.cu:27-69)
+// gann_search ~ GustANN::search -> PureMemExecutor::search            (src/pure_mem.cu:71-199)
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "gann_internal.h"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int set_error(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+struct CudaFail {
+  cudaError_t e;
+  const char* what;
+};
+
+void ck(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw CudaFail{e, what};
+}
+
+template <class T>
+T* dev_alloc(gann_index* h, size_t count) {
+  void* p = nullptr;
+  if (count == 0) count = 1;
+  cudaError_t e = cudaMalloc(&p, sizeof(T) * count);
+  if (e != cudaSuccess) throw CudaFail{e, "cudaMalloc"};
+  h->allocations.push_back(p);
+  h->device_bytes += (int64_t)(sizeof(T) * count);
+  return static_cast<T*>(p);
+}
+
+template <class T>
+T* upload(gann_index* h, const std::vector<T>& v) {
+  T* d = dev_alloc<T>(h, v.size());
+  if (!v.empty()) ck(cudaMemcpy(d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice), "upload");
+  return d;
+}
+
+// Stream the page body of _disk.index (everything after the first 4 KB sector,
+// src/pure_mem.cu:51-61) into HBM through two pinned bounce buffers.
+void upload_pages(gann_index* h, const std::string& path, uint8_t* dst, int64_t bytes) {
+  FILE* f = std::fopen(path.c_str(), "rb");
+  if (!f) throw gann::GannError{GANN_EIO, "cannot open " + path};
+  std::unique_ptr<FILE, int (*)(FILE*)> guard(f, std::fclose);
+  std::fseek(f, gann::kPageSize, SEEK_SET);
+  const size_t chunk = 64u << 20;
+  uint8_t* bounce[2] = {nullptr, nullptr};
+  cudaEvent_t done[2];
+  ck(cudaMallocHost(&bounce[0], chunk), "cudaMallocHost");
+  if (cudaMallocHost(&bounce[1], chunk) != cudaSuccess) {
+    cudaFreeHost(bounce[0]);
+    throw CudaFail{cudaErrorMemoryAllocation, "cudaMallocHost"};
+  }
+  cudaEventCreateWithFlags(&done[0], cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&done[1], cudaEventDisableTiming);
+  bool used[2] = {false, false};
+  int64_t off = 0;
+  int b = 0;
+  std::string err;
+  while (off < bytes) {
+    size_t n = (size_t)std::min<int64_t>(chunk, bytes - off);
+    if (used[b]) cudaEventSynchronize(done[b]);
+    if (std::fread(bounce[b], 1, n, f) != n) {
+      err = "short read of index pages: " + path;
+      break;
+    }
+    if (cudaMemcpyAsync(dst + off, bounce[b], n, cudaMemcpyHostToDevice, h->stream) != cudaSuccess ||
+        cudaEventRecord(done[b], h->stream) != cudaSuccess) {
+      err = "page upload failed";
+      break;
+    }
+    used[b] = true;
+    off += (int64_t)n;
+    b ^= 1;
+  }
+  cudaStreamSynchronize(h->stream);
+  cudaEventDestroy(done[0]);
+  cudaEventDestroy(done[1]);
+  cudaFreeHost(bounce[0]);
+  cudaFreeHost(bounce[1]);
+  if (!err.empty()) throw gann::GannError{GANN_EIO, err};
+}
+
+// Load-time check of every record: degree <= max_m0 and neighbour ids in [0, n).
+__global__ void validate_records(const uint8_t* pages, int64_t n, int64_t npp, int64_t node_len,
+                                 int64_t data_len, int max_m, unsigned long long* bad) {
+  for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < n; u += (int64_t)gridDim.x * blockDim.x) {
+    const uint8_t* node = pages + (u / npp) * gann::kPageSize + (u % npp) * node_len;
+    const int32_t* meta = reinterpret_cast<const int32_t*>(node + data_len);
+    int deg = meta[0];
+    bool ok = deg >= 0 && deg <= max_m;
+    for (int t = 0; ok && t < deg; t++) ok = (unsigned)meta[1 + t] < (unsigned)n;
+    if (!ok) atomicAdd(bad, 1ull);
+  }
+}
+
+void free_all(gann_index* h) {
+  for (void* p : h->allocations) cudaFree(p);
+  h->allocations.clear();
+  for (void* p : {(void*)h->d_q, (void*)h->d_nns, (void*)h->d_dists, (void*)h->d_found})
+    if (p) cudaFree(p);
+  h->d_q = nullptr;
+  h->d_nns = nullptr;
+  h->d_dists = nullptr;
+  h->d_found = nullptr;
+  if (h->ev0) cudaEventDestroy(h->ev0);
+  if (h->ev1) cudaEventDestroy(h->ev1);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  h->ev0 = h->ev1 = nullptr;
+  h->stream = nullptr;
+}
+
+template <class T>
+void grow(T*& p, size_t& cap, size_t need) {
+  if (need <= cap) return;
+  if (p) cudaFree(p);
+  p = nullptr;
+  cap = 0;
+  ck(cudaMalloc(&p, sizeof(T) * need), "cudaMalloc (search buffers)");
+  cap = need;
+}
+
+int check_search_args(const gann_index* h, int nq, int topk, int ef_search) {
+  if (!h) return set_error(GANN_EINVAL, "null handle");
+  if (nq < 0) return set_error(GANN_EINVAL, "nq must be >= 0");
+  if (topk < 1 || ef_search < 1) return set_error(GANN_EINVAL, "topk and ef_search must be >= 1");
+  if (ef_search > 4096 || topk > 4096) return set_error(GANN_ERANGE, "topk and ef_search are limited to 4096");
+  size_t per_warp = gann::plain_smem_per_warp(h->hx.pq_m, ef_search, (int)h->hx.max_m0, topk, (int)h->hx.dim);
+  if (per_warp > 227 * 1024)
+    return set_error(GANN_ERANGE, "table + lists of one query exceed the 227 KB of shared memory per CTA");
+  return GANN_OK;
+}
+
+gann::PlainParams make_params(gann_index* h, const float* d_q, int nq, int topk, int ef_search, int32_t* d_nns,
+                              float* d_dists, int32_t* d_found) {
+  gann::PlainParams p{};
+  p.ix = h->dx;
+  p.n = h->hx.n;
+  p.npp = h->hx.npp;
+  p.node_len = h->hx.node_len;
+  p.data_len = h->hx.data_len;
+  p.medoid = h->hx.medoid;
+  p.dim = (int)h->hx.dim;
+  p.max_m = (int)h->hx.max_m0;
+  p.M = h->hx.pq_m;
+  p.has_nav = h->hx.has_nav;
+  p.nav_n = h->hx.nav_n;
+  p.nav_max_m = h->hx.nav_max_m;
+  p.nav_start = h->hx.nav_start;
+  p.queries = d_q;
+  p.nq = nq;
+  p.L = ef_search;
+  p.k = topk;
+  p.fma_table = h->fma_table;
+  p.fma_exact = h->fma_exact;
+  p.nns = d_nns;
+  p.dists = d_dists;
+  p.found = d_found;
+  p.hops = nullptr;
+  p.next_query = h->d_counter;
+  p.err = h->d_err;
+  return p;
+}
+
+int kernel_error_status(unsigned int err) {
+  if (!err) return GANN_OK;
+  std::string m = "search kernel reported:";
+  if (err & gann::kErrBadId) m += " neighbour/entry id out of range;";
+  if (err & gann::kErrBadDegree) m += " degree word above max_m0;";
+  if (err & gann::kErrHopCap) m += " hop limit reached;";
+  if (err & gann::kErrNavCap) m += " pivot-graph iteration limit reached;";
+  if (err & gann::kErrWaitLimit) m += " wait limit reached;";
+  return set_error(GANN_EKERNEL, m);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* gann_last_error(void) { return g_last_error.c_str(); }
+
+int gann_open(const char* index_file, const char* pq_prefix, const char* nav_dir, int dtype, int flags,
+              gann_t** out) {
+  if (!out) return set_error(GANN_EINVAL, "null output handle");
+  *out = nullptr;
+  if (!index_file || !pq_prefix) return set_error(GANN_EINVAL, "index_file and pq_prefix are required");
+  if (dtype != GANN_UINT8 && dtype != GANN_FLOAT) return set_error(GANN_EINVAL, "dtype must be GANN_UINT8 or GANN_FLOAT");
+  auto h = std::make_unique<gann_index>();
+  try {
+    h->hx.dtype = dtype;
+    h->hx.elt = dtype == GANN_UINT8 ? 1 : 4;
+    gann::read_disk_index(index_file, h->hx, nullptr);
+    std::vector<uint8_t> codes;
+    gann::read_pq(pq_prefix, h->hx, codes);
+    if ((int64_t)h->hx.pivots.size() / gann::kPivots != h->hx.dim)
+      throw gann::GannError{GANN_EFORMAT, "PQ pivots dimension differs from the index dimension"};
+    if (nav_dir && nav_dir[0]) gann::read_nav(nav_dir, h->hx);
+
+    ck(cudaGetDevice(&h->device), "cudaGetDevice");
+    ck(cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device), "cudaDeviceGetAttribute");
+    ck(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    ck(cudaEventCreate(&h->ev0), "cudaEventCreate");
+    ck(cudaEventCreate(&h->ev1), "cudaEventCreate");
+
+    const gann::HostIndex& hx = h->hx;
+    uint8_t* pages = dev_alloc<uint8_t>(h.get(), (size_t)hx.num_pages * gann::kPageSize);
+    upload_pages(h.get(), index_file, pages, hx.num_pages * (int64_t)gann::kPageSize);
+    h->dx.pages = pages;
+    h->dx.codes = upload(h.get(), codes);
+    std::vector<float> pivots_t((size_t)hx.dim * gann::kPivots);  // pq_search.cu:86-91
+    for (int i = 0; i < gann::kPivots; i++)
+      for (int64_t j = 0; j < hx.dim; j++) pivots_t[j * gann::kPivots + i] = hx.pivots[i * hx.dim + j];
+    h->dx.pivots_t = upload(h.get(), pivots_t);
+    h->dx.centroid = upload(h.get(), hx.centroid);
+    h->dx.chunk_off = upload(h.get(), hx.chunk_offsets);
+    if (hx.has_nav) {
+      h->dx.nav_data = upload(h.get(), hx.nav_data);
+      h->dx.nav_graph = upload(h.get(), hx.nav_graph);
+      h->dx.nav_map = upload(h.get(), hx.nav_map);
+    }
+    h->d_counter = dev_alloc<int>(h.get(), 1);
+    h->d_err = dev_alloc<unsigned int>(h.get(), 1);
+    ck(cudaMemset(h->d_err, 0, sizeof(unsigned int)), "cudaMemset");
+    if (!(flags & GANN_OPEN_NO_VALIDATE)) {
+      unsigned long long* bad = dev_alloc<unsigned long long>(h.get(), 1);
+      ck(cudaMemsetAsync(bad, 0, sizeof(*bad), h->stream), "cudaMemset");
+      validate_records<<<h->num_sms * 8, 256, 0, h->stream>>>(pages, hx.n, hx.npp, hx.node_len, hx.data_len,
+                                                              (int)hx.max_m0, bad);
+      ck(cudaGetLastError(), "validate launch");
+      unsigned long long nbad = 0;
+      ck(cudaMemcpyAsync(&nbad, bad, sizeof(nbad), cudaMemcpyDeviceToHost, h->stream), "cudaMemcpy");
+      ck(cudaStreamSynchronize(h->stream), "validate");
+      if (nbad)
+        throw gann::GannError{GANN_EFORMAT, std::to_string(nbad) +
+                                                " records have a degree above max_m0 or a neighbour id outside the index"};
+    }
+    ck(cudaStreamSynchronize(h->stream), "open");
+  } catch (const gann::GannError& e) {
+    free_all(h.get());
+    return set_error(e.code, e.msg);
+  } catch (const CudaFail& e) {
+    free_all(h.get());
+    return set_error(e.e == cudaErrorMemoryAllocation ? GANN_ENOMEM : GANN_ECUDA,
+                     std::string(e.what) + ": " + cudaGetErrorString(e.e));
+  } catch (const std::bad_alloc&) {
+    free_all(h.get());
+    return set_error(GANN_ENOMEM, "host allocation failed");
+  }
+  *out = h.release();
+  return GANN_OK;
+}
+
+int gann_close(gann_t* h) {
+  if (!h) return GANN_OK;
+  {
+    std::lock_guard<std::mutex> lk(h->mu);
+    int prev = -1;
+    cudaGetDevice(&prev);
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    free_all(h);
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+  delete h;
+  return GANN_OK;
+}
+
+int gann_get_info(const gann_t* h, gann_info_t* out) {
+  if (!h || !out) return set_error(GANN_EINVAL, "null argument");
+  const gann::HostIndex& hx = h->hx;
+  out->num_points = hx.n;
+  out->dim = hx.dim;
+  out->max_degree = hx.max_m0;
+  out->medoid = hx.medoid;
+  out->node_len = hx.node_len;
+  out->nodes_per_page = hx.npp;
+  out->num_pages = hx.num_pages;
+  out->pq_chunks = hx.pq_m;
+  out->dtype = hx.dtype;
+  out->has_nav = hx.has_nav;
+  out->nav_points = hx.nav_n;
+  out->nav_max_degree = hx.nav_max_m;
+  out->device = h->device;
+  out->device_bytes = h->device_bytes;
+  return GANN_OK;
+}
+
+int gann_search_device(gann_t* h, const float* d_queries, int nq, int topk, int ef_search, int32_t* d_nns,
+                       float* d_distances, int32_t* d_found_cnt, void* stream) {
+  int rc = check_search_args(h, nq, topk, ef_search);
+  if (rc) return rc;
+  if (nq == 0) return GANN_OK;
+  if (!d_queries || !d_nns || !d_distances || !d_found_cnt) return set_error(GANN_EINVAL, "null buffer");
+  std::lock_guard<std::mutex> lk(h->mu);
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
+  gann::PlainParams p = make_params(h, d_queries, nq, topk, ef_search, d_nns, d_distances, d_found_cnt);
+  cudaError_t e = cudaMemsetAsync(h->d_counter, 0, sizeof(int), s);
+  if (e == cudaSuccess) e = gann::launch_plain(p, h->hx.dtype, h->num_sms, s);
+  if (e != cudaSuccess) return set_error(GANN_ECUDA, std::string("plain search launch: ") + cudaGetErrorString(e));
+  return GANN_OK;
+}
+
+int gann_search(gann_t* h, const float* queries, int nq, int topk, int ef_search, int32_t* nns, float* distances,
+                int32_t* found_cnt, double* run_time) {
+  int rc = check_search_args(h, nq, topk, ef_search);
+  if (rc) return rc;
+  if (run_time) *run_time = 0.0;
+  if (nq == 0) return GANN_OK;
+  if (!queries || !nns || !distances || !found_cnt) return set_error(GANN_EINVAL, "null buffer");
+  std::lock_guard<std::mutex> lk(h->mu);
+  try {
+    const size_t qn = (size_t)nq * h->hx.dim, on = (size_t)nq * topk;
+    grow(h->d_q, h->cap_q, qn);
+    grow(h->d_nns, h->cap_out, on);
+    grow(h->d_dists, h->cap_dists, on);
+    grow(h->d_found, h->cap_found, (size_t)nq);
+    cudaStream_t s = h->stream;
+    ck(cudaMemcpyAsync(h->d_q, queries, sizeof(float) * qn, cudaMemcpyHostToDevice, s), "query upload");
+    gann::PlainParams p = make_params(h, h->d_q, nq, topk, ef_search, h->d_nns, h->d_dists, h->d_found);
+    ck(cudaMemsetAsync(h->d_counter, 0, sizeof(int), s), "cudaMemset");
+    ck(cudaEventRecord(h->ev0, s), "cudaEventRecord");
+    ck(gann::launch_plain(p, h->hx.dtype, h->num_sms, s), "plain search launch");
+    ck(cudaEventRecord(h->ev1, s), "cudaEventRecord");
+    ck(cudaMemcpyAsync(nns, h->d_nns, sizeof(int32_t) * on, cudaMemcpyDeviceToHost, s), "result download");
+    ck(cudaMemcpyAsync(distances, h->d_dists, sizeof(float) * on, cudaMemcpyDeviceToHost, s), "result download");
+    ck(cudaMemcpyAsync(found_cnt, h->d_found, sizeof(int32_t) * nq, cudaMemcpyDeviceToHost, s), "result download");
+    unsigned int err = 0;
+    ck(cudaMemcpyAsync(&err, h->d_err, sizeof(err), cudaMemcpyDeviceToHost, s), "error word");
+    ck(cudaStreamSynchronize(s), "search");
+    if (err) {
+      ck(cudaMemset(h->d_err, 0, sizeof(unsigned int)), "cudaMemset");
+      return kernel_error_status(err);
+    }
+    float ms = 0.0f;
+    ck(cudaEventElapsedTime(&ms, h->ev0, h->ev1), "cudaEventElapsedTime");
+    if (run_time) *run_time = ms * 1e-3;
+  } catch (const CudaFail& e) {
+    return set_error(GANN_ECUDA, std::string(e.what) + ": " + cudaGetErrorString(e.e));
+  }
+  return GANN_OK;
+}
+
+/* Synchronise `stream` (NULL = the handle's stream) and report any error word
+ * left by kernels launched with gann_search_device; clears it. */
+int gann_check(gann_t* h, void* stream) {
+  if (!h) return set_error(GANN_EINVAL, "null handle");
+  std::lock_guard<std::mutex> lk(h->mu);
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
+  unsigned int err = 0;
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) e = cudaMemcpy(&err, h->d_err, sizeof(err), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return set_error(GANN_ECUDA, std::string("gann_check: ") + cudaGetErrorString(e));
+  if (err) {
+    cudaMemset(h->d_err, 0, sizeof(unsigned int));
+    return kernel_error_status(err);
+  }
+  return GANN_OK;
+}
+
+/* Select the FMA behaviour of the plain form at the two reference sites
+ * (src/impl/pq.cuh:40 table accumulate, src/impl/util.cuh:37 exact distance).
+ * Both default to 1 (fused); tests/golden pins that choice against the
+ * reference's own build. */
+int gann_set_fma(gann_t* h, int fma_table, int fma_exact) {
+  if (!h) return set_error(GANN_EINVAL, "null handle");
+  std::lock_guard<std::mutex> lk(h->mu);
+  h->fma_table = fma_table ? 1 : 0;
+  h->fma_exact = fma_exact ? 1 : 0;
+  return GANN_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,111 @@
+// Internal types shared by the host side and the kernels of libgann.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/gann.h"
+
+namespace gann {
+
+constexpr int kPageSize = 4096;  // PureMemExecutor::PAGE_SIZE, src/pure_mem.hpp:25
+constexpr int kPivots = 256;     // PQSearchData::num_pivots, src/pq_search.hpp:12
+constexpr uint32_t kMask = 0x7fffffffu;
+constexpr uint32_t kExpanded = 0x80000000u;
+
+// Error word bits written by kernels (device -> host).
+enum : uint32_t {
+  kErrBadId = 1u,       // neighbour or entry id outside [0, n)
+  kErrBadDegree = 2u,   // degree word larger than max_m0
+  kErrHopCap = 4u,      // walk exceeded its hop limit
+  kErrNavCap = 8u,      // pivot-graph walk exceeded its iteration limit
+  kErrWaitLimit = 16u,  // a bounded spin-wait gave up
+};
+
+// Host copy of the index files, parsed and checked (gann_io.cpp).
+struct HostIndex {
+  int dtype = 0;  // GANN_UINT8 / GANN_FLOAT
+  int elt = 1;
+  int64_t n = 0, dim = 0, medoid = 0, node_len = 0, npp = 0, max_m0 = 0, data_len = 0,
+          num_pages = 0;
+  int pq_m = 0;
+  std::vector<float> pivots;          // 256 x dim (row = pivot)
+  std::vector<float> centroid;        // dim
+  std::vector<int32_t> chunk_offsets; // M + 1, contiguous ranges covering [0, dim)
+  bool has_nav = false;
+  int nav_n = 0, nav_max_m = 0, nav_start = 0;
+  std::vector<uint8_t> nav_data;   // nav_n x dim x elt
+  std::vector<int32_t> nav_graph;  // nav_n x nav_max_m, -1 padded
+  std::vector<int32_t> nav_map;    // nav_n
+};
+
+// Device-resident index (HBM layout).
+struct DeviceIndex {
+  const uint8_t* pages = nullptr;   // num_pages x 4096, the _disk.index body
+  const uint8_t* codes = nullptr;   // n x M PQ codes
+  const float* pivots_t = nullptr;  // dim x 256 (transposed pivots)
+  const float* centroid = nullptr;  // dim
+  const int32_t* chunk_off = nullptr;  // M + 1
+  const uint8_t* nav_data = nullptr;   // nav_n x dim x elt
+  const int32_t* nav_graph = nullptr;  // nav_n x nav_max_m
+  const int32_t* nav_map = nullptr;    // nav_n
+};
+
+// Launch parameters of the plain search kernel (walk_plain.cu).
+struct PlainParams {
+  DeviceIndex ix;
+  int64_t n, npp, node_len, data_len, medoid;
+  int dim, max_m, M;
+  int has_nav, nav_n, nav_max_m, nav_start;
+  const float* queries;  // nq x dim
+  int nq, L, k;
+  int fma_table, fma_exact;  // FMA at pq.cuh:40 / util.cuh:37
+  int32_t* nns;              // nq x k
+  float* dists;              // nq x k
+  int32_t* found;            // nq
+  int32_t* hops;             // nq or null
+  int* next_query;           // work counter, zeroed before launch
+  unsigned int* err;         // error word
+};
+
+// Per-warp shared-memory footprint of the plain kernel, in bytes.
+size_t plain_smem_per_warp(int M, int L, int max_m, int k, int dim);
+// Launch the plain kernel for one batch (walk_plain.cu). Returns a cudaError_t.
+cudaError_t launch_plain(const PlainParams& p, int dtype, int num_sms, cudaStream_t stream);
+
+// File readers (gann_io.cpp). Throw GannError on failure.
+void read_disk_index(const std::string& path, HostIndex& hx, std::vector<uint8_t>* pages_out);
+void read_pq(const std::string& prefix, HostIndex& hx, std::vector<uint8_t>& codes);
+void read_nav(const std::string& dir, HostIndex& hx);
+
+struct GannError {
+  int code;
+  std::string msg;
+};
+
+}  // namespace gann
+
+struct gann_index {
+  std::mutex mu;
+  gann::HostIndex hx;
+  gann::DeviceIndex dx;
+  int device = 0;
+  int num_sms = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::vector<void*> allocations;  // device allocations owned by the handle
+  int64_t device_bytes = 0;
+  int* d_counter = nullptr;        // work counter scratch (plain kernel)
+  unsigned int* d_err = nullptr;   // kernel error word
+  // per-call device buffers, grown on demand
+  float* d_q = nullptr;
+  int32_t* d_nns = nullptr;
+  float* d_dists = nullptr;
+  int32_t* d_found = nullptr;
+  size_t cap_q = 0, cap_out = 0, cap_dists = 0, cap_found = 0;
+  int fma_table = 1, fma_exact = 1;
+};

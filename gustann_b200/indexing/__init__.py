@@ -1,0 +1,85 @@
+"""Index preparation: synthetic data, graph + PQ + pivot-graph build, file writers.
+
+``build_index`` produces the reference's input files (the ones
+``GustANN::init_pure_mem`` reads, src/ssd_search.cu:55-79) from a base matrix:
+
+    <out>/index_disk.index
+    <out>/index_pq_pivots.bin, <out>/index_pq_compressed.bin
+    <out>/nav/{nav_index, nav_index.data, map.txt}
+
+The pivot graph follows scripts/gen_pivot_graph.sh:7-14: a uniform sample of
+the base (bin/gen_small_file.cpp's shuffle), indexed with R=32.
+"""
+from __future__ import annotations
+
+import os
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import builder, formats, pq, synth  # noqa: F401
+
+
+@dataclass
+class IndexFiles:
+    index_file: str
+    pq_prefix: str
+    nav_dir: str | None
+    n: int
+    dim: int
+    dtype: str
+    R: int
+    M: int
+    medoid: int
+    timings: dict = field(default_factory=dict)
+
+
+def _np(x):
+    return x.cpu().numpy() if isinstance(x, torch.Tensor) else np.asarray(x)
+
+
+def build_index(base, out_dir: str, R: int, M: int = 32, alpha: float = 1.2, nav_samples: int | None = None,
+                nav_R: int = 32, device=None, n_coarse: int | None = None, nprobe: int = 4,
+                pq_train: int = 1 << 18, seed: int = 7, legacy_pq: bool = False) -> IndexFiles:
+    """Build and write every file of one index. ``base`` is an n x dim uint8 or
+    float32 array/tensor. ``nav_samples`` = 0 writes no pivot graph."""
+    from .. import sample_pivots
+
+    t0 = time.time()
+    timings = {}
+    os.makedirs(out_dir, exist_ok=True)
+    x = base if isinstance(base, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(base))
+    if device is not None:
+        x = x.to(device)
+    n, dim = x.shape
+    kind = "u8" if x.dtype == torch.uint8 else "f32"
+    g, deg, med = builder.build(x, R, alpha, n_coarse=n_coarse, nprobe=nprobe, seed=seed)
+    timings["graph_s"] = time.time() - t0
+    t1 = time.time()
+    pivots, centroid, offs = pq.train(x, M, n_train=pq_train, seed=seed + 4)
+    codes = pq.encode(x, pivots, centroid, offs)
+    timings["pq_s"] = time.time() - t1
+    t2 = time.time()
+    index_file = os.path.join(out_dir, "index_disk.index")
+    pq_prefix = os.path.join(out_dir, "index_pq")
+    data_np = _np(x)
+    formats.write_disk_index(index_file, data_np, g, deg, med, R)
+    formats.write_pq(pq_prefix, pivots, centroid, offs, codes, legacy=legacy_pq)
+    timings["write_s"] = time.time() - t2
+    nav_dir = None
+    if nav_samples is None:
+        nav_samples = max(64, n // 100)
+    if nav_samples:
+        t3 = time.time()
+        ids = sample_pivots(n, min(nav_samples, n))
+        sub = x[torch.from_numpy(ids.astype(np.int64)).to(x.device)]
+        ng, ndeg, nmed = builder.build(sub, nav_R, alpha, seed=seed + 1)
+        if int(ndeg.min()) < 3:
+            raise RuntimeError("pivot graph has a node with fewer than 3 neighbours")
+        nav_dir = os.path.join(out_dir, "nav")
+        formats.write_nav(nav_dir, _np(sub), ng, ndeg, nmed, ids)
+        timings["nav_s"] = time.time() - t3
+    timings["total_s"] = time.time() - t0
+    return IndexFiles(index_file, pq_prefix, nav_dir, n, dim, kind, R, M, med, timings)

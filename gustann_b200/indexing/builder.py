@@ -1,0 +1,240 @@
+"""Vamana-style graph builder (torch, CPU or GPU).
+
+The reference builds its graphs with DiskANN (``build_disk_index -R -L``,
+scripts/build_diskann_index.sh:7; ``build_memory_index -R 32 -L 50`` for the
+pivot graph, scripts/gen_pivot_graph.sh:7-14). DiskANN is an empty submodule
+here, so this module produces graphs of the same kind for the reference's file
+formats. Search parity is defined on a given index file, so the builder only has
+to produce valid, navigable graphs; it is not meant to match DiskANN edge for
+edge.
+
+Algorithm (GPU-friendly restatement of Vamana's pruning):
+1. candidates: exact k-nearest neighbours for small n; for large n, points are
+   grouped by a coarse k-means and each group searches the members of its
+   ``nprobe`` nearest groups;
+2. RobustPrune with ``alpha`` on squared L2 (a candidate c is dropped when an
+   already kept neighbour j has alpha * d(j, c) < d(p, c));
+3. reverse edges: each kept edge p->q offers q->p; rows that overflow R are
+   pruned again with the same rule.
+The medoid is the point nearest to the mean (DiskANN's entry point).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import torch
+
+
+def _f32(x: torch.Tensor) -> torch.Tensor:
+    return x if x.dtype == torch.float32 else x.float()
+
+
+def sqdist(a: torch.Tensor, b: torch.Tensor, an: torch.Tensor | None = None, bn: torch.Tensor | None = None):
+    """Squared L2 between rows of a (m x d) and b (n x d), FP32 (exact for uint8 data, d <= 128)."""
+    a = _f32(a)
+    b = _f32(b)
+    if an is None:
+        an = (a * a).sum(1)
+    if bn is None:
+        bn = (b * b).sum(1)
+    d = an[:, None] + bn[None, :] - 2.0 * (a @ b.T)
+    return d.clamp_min_(0.0)
+
+
+def medoid(x: torch.Tensor, chunk: int = 1 << 20) -> int:
+    mean = torch.zeros(x.shape[1], dtype=torch.float64, device=x.device)
+    for s in range(0, x.shape[0], chunk):
+        mean += _f32(x[s:s + chunk]).double().sum(0)
+    mean = (mean / x.shape[0]).float()
+    best, best_d = 0, math.inf
+    for s in range(0, x.shape[0], chunk):
+        d = ((_f32(x[s:s + chunk]) - mean) ** 2).sum(1)
+        v, i = torch.min(d, 0)
+        if float(v) < best_d:
+            best_d, best = float(v), s + int(i)
+    return best
+
+
+def kmeans(x: torch.Tensor, k: int, iters: int, seed: int, sample: int = 1 << 18) -> torch.Tensor:
+    """Plain Lloyd k-means on a seeded sample; returns k x d FP32 centres."""
+    g = torch.Generator(device="cpu")
+    g.manual_seed(seed)
+    n = x.shape[0]
+    idx = torch.randperm(n, generator=g)[: min(n, sample)].to(x.device)
+    s = _f32(x[idx])
+    cent = s[torch.randperm(s.shape[0], generator=g)[:k].to(x.device)].clone()
+    for _ in range(iters):
+        lab = assign(s, cent)
+        sums = torch.zeros_like(cent).index_add_(0, lab, s)
+        cnt = torch.bincount(lab, minlength=k).float()
+        empty = cnt == 0
+        cent = torch.where(empty[:, None], cent, sums / cnt.clamp_min(1)[:, None])
+    return cent
+
+
+def assign(x: torch.Tensor, cent: torch.Tensor, chunk: int = 1 << 16) -> torch.Tensor:
+    cn = (cent * cent).sum(1)
+    out = torch.empty(x.shape[0], dtype=torch.long, device=x.device)
+    for s in range(0, x.shape[0], chunk):
+        out[s:s + chunk] = sqdist(x[s:s + chunk], cent, bn=cn).argmin(1)
+    return out
+
+
+def knn_candidates(x: torch.Tensor, K: int, n_coarse: int | None = None, nprobe: int = 4, seed: int = 7,
+                   block: int = 4096) -> tuple[torch.Tensor, torch.Tensor]:
+    """K nearest (approximate for large n) neighbours of every point, self excluded.
+    Returns (ids n x K int64, squared distances n x K), rows sorted by distance; -1 pads."""
+    n = x.shape[0]
+    dev = x.device
+    K = min(K, n - 1)
+    xn = (_f32(x) ** 2).sum(1) if n <= (1 << 22) else None
+    ids = torch.full((n, K), -1, dtype=torch.long, device=dev)
+    dis = torch.full((n, K), float("inf"), dtype=torch.float32, device=dev)
+    if n_coarse is None:
+        n_coarse = 1 if n <= 50_000 else max(1, n // 1000)
+    if n_coarse == 1:
+        for s in range(0, n, block):
+            e = min(n, s + block)
+            d = sqdist(x[s:e], x, an=None if xn is None else xn[s:e], bn=xn)
+            d[torch.arange(e - s, device=dev), torch.arange(s, e, device=dev)] = float("inf")
+            v, i = torch.topk(d, K, dim=1, largest=False)
+            ids[s:e], dis[s:e] = i, v
+        return ids, dis
+    cent = kmeans(x, n_coarse, iters=8, seed=seed)
+    lab = assign(x, cent)
+    order = torch.argsort(lab)
+    counts = torch.bincount(lab, minlength=n_coarse)
+    starts = torch.cumsum(counts, 0) - counts
+    near = torch.topk(sqdist(cent, cent), min(nprobe, n_coarse), dim=1, largest=False).indices
+    counts_h, starts_h, near_h = counts.cpu().numpy(), starts.cpu().numpy(), near.cpu().numpy()
+    for c in range(n_coarse):
+        if counts_h[c] == 0:
+            continue
+        mem = order[starts_h[c]: starts_h[c] + counts_h[c]]
+        pool = torch.cat([order[starts_h[o]: starts_h[o] + counts_h[o]] for o in near_h[c]])
+        kk = min(K, pool.numel() - 1)
+        for s in range(0, mem.numel(), block):
+            m = mem[s:s + block]
+            d = sqdist(x[m], x[pool])
+            d[m[:, None] == pool[None, :]] = float("inf")
+            v, i = torch.topk(d, kk, dim=1, largest=False)
+            ids[m, :kk] = pool[i]
+            dis[m, :kk] = v
+    return ids, dis
+
+
+def robust_prune(x: torch.Tensor, cand: torch.Tensor, cand_d: torch.Tensor, R: int, alpha: float,
+                 batch: int = 8192) -> torch.Tensor:
+    """RobustPrune over rows of candidates sorted by distance (-1 = none).
+    Returns n x R int64 neighbour ids (-1 padded), kept in candidate order."""
+    n, K = cand.shape
+    out = torch.full((n, R), -1, dtype=torch.long, device=x.device)
+    for s in range(0, n, batch):
+        e = min(n, s + batch)
+        c = cand[s:e]
+        cd = cand_d[s:e]
+        valid = c >= 0
+        V = _f32(x[c.clamp_min(0)])
+        vn = (V * V).sum(-1)
+        D = (vn[:, :, None] + vn[:, None, :] - 2.0 * torch.bmm(V, V.transpose(1, 2))).clamp_min_(0.0)
+        alive = valid.clone()
+        keep = torch.zeros_like(valid)
+        count = torch.zeros(e - s, dtype=torch.long, device=x.device)
+        col = torch.arange(K, device=x.device)
+        for j in range(K):
+            sel = alive[:, j] & (count < R)
+            if not bool(sel.any()):
+                if not bool(alive[:, j:].any()):
+                    break
+                continue
+            keep[:, j] = sel
+            count += sel.long()
+            kill = sel[:, None] & (alpha * D[:, j, :] < cd) & (col[None, :] > j)
+            alive &= ~kill
+        pos = torch.cumsum(keep.long(), 1) - 1
+        rows = torch.arange(e - s, device=x.device)[:, None].expand(-1, K)
+        m = keep & (pos < R)
+        out[s:e][rows[m], pos[m]] = c[m]
+    return out
+
+
+def _dedupe_sorted(ids: torch.Tensor, d: torch.Tensor):
+    """Sort rows by (distance, id) and blank out repeated ids (-1, inf)."""
+    ids = ids.clone()
+    d = d.clone()
+    d[ids < 0] = float("inf")
+    o = torch.argsort(ids, dim=1, stable=True)
+    ids = torch.gather(ids, 1, o)
+    d = torch.gather(d, 1, o)
+    dup = torch.zeros_like(ids, dtype=torch.bool)
+    dup[:, 1:] = (ids[:, 1:] == ids[:, :-1]) & (ids[:, 1:] >= 0)
+    ids[dup] = -1
+    d[dup | (ids < 0)] = float("inf")
+    o = torch.argsort(d, dim=1, stable=True)
+    return torch.gather(ids, 1, o), torch.gather(d, 1, o)
+
+
+def add_reverse_edges(x: torch.Tensor, g: torch.Tensor, R: int, alpha: float, in_cap: int | None = None,
+                      batch: int = 8192) -> torch.Tensor:
+    """Offer every edge p->q back as q->p; rows that overflow R are pruned again."""
+    n = g.shape[0]
+    dev = x.device
+    in_cap = in_cap or R
+    src = torch.arange(n, device=dev)[:, None].expand(-1, g.shape[1])
+    m = g >= 0
+    rs, rd = g[m], src[m]  # reverse edge rs -> rd
+    o = torch.argsort(rs, stable=True)
+    rs, rd = rs[o], rd[o]
+    cnt = torch.bincount(rs, minlength=n)
+    start = torch.cumsum(cnt, 0) - cnt
+    rank = torch.arange(rs.numel(), device=dev) - start[rs]
+    keep = rank < in_cap
+    inc = torch.full((n, in_cap), -1, dtype=torch.long, device=dev)
+    inc[rs[keep], rank[keep]] = rd[keep]
+    out = torch.full((n, R), -1, dtype=torch.long, device=dev)
+    for s in range(0, n, batch):
+        e = min(n, s + batch)
+        cand = torch.cat([g[s:e], inc[s:e]], 1)
+        V = _f32(x[cand.clamp_min(0)])
+        p = _f32(x[s:e])[:, None, :]
+        d = ((V - p) ** 2).sum(-1)
+        cand, d = _dedupe_sorted(cand, d)
+        nuniq = (cand >= 0).sum(1)
+        small = nuniq <= R
+        rows = out[s:e]
+        rows[small] = cand[small, :R]
+        if bool((~small).any()):
+            big = torch.nonzero(~small).squeeze(1)
+            rows[big] = robust_prune(x, cand[big], d[big], R, alpha, batch=batch)
+        out[s:e] = rows
+    return out
+
+
+def build(x: torch.Tensor, R: int, alpha: float = 1.2, K: int | None = None, n_coarse: int | None = None,
+          nprobe: int = 4, seed: int = 7) -> tuple[np.ndarray, np.ndarray, int]:
+    """Build a graph over the rows of ``x`` (uint8 or float32 tensor).
+    Returns (adjacency n x R int32 padded with -1, degrees n int32, medoid)."""
+    K = K or 2 * R
+    cand, cand_d = knn_candidates(x, K, n_coarse=n_coarse, nprobe=nprobe, seed=seed)
+    g = robust_prune(x, cand, cand_d, R, alpha)
+    g = add_reverse_edges(x, g, R, alpha)
+    deg = (g >= 0).sum(1)
+    return (g.to(torch.int32).cpu().numpy(), deg.to(torch.int32).cpu().numpy(), medoid(x))
+
+
+def reachable_from(graph: np.ndarray, degrees: np.ndarray, start: int) -> np.ndarray:
+    """Boolean mask of nodes reachable from ``start`` by breadth-first search."""
+    n = graph.shape[0]
+    seen = np.zeros(n, dtype=bool)
+    seen[start] = True
+    frontier = np.array([start])
+    mask = np.arange(graph.shape[1])[None, :]
+    while frontier.size:
+        rows = graph[frontier]
+        nb = rows[mask < degrees[frontier][:, None]]
+        nb = np.unique(nb[nb >= 0])
+        nb = nb[~seen[nb]]
+        seen[nb] = True
+        frontier = nb
+    return seen

@@ -1,0 +1,137 @@
+/*
+ * gann.h -- C ABI of the B200-native GustANN all-in-GPU search path.
+ *
+ * Drop-in for the reference's `search_mem -G` entry points. Each declaration
+ * cites the reference interface it replaces (paths relative to the GustANN
+ * project root). All calls return a status (GANN_OK = 0); on failure
+ * gann_last_error() describes the cause (the reference aborts, exits or throws
+ * instead, src/common.hpp:17, src/common_cuda.cuh:10-17).
+ *
+ * Threading: a handle may be used from several host threads; calls on one
+ * handle are serialised internally. Each handle lives on the CUDA device that
+ * was current when it was opened and issues its work on its own stream.
+ */
+#ifndef GANN_H_
+#define GANN_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct gann_index gann_t;
+
+/* status codes */
+enum {
+  GANN_OK = 0,
+  GANN_EINVAL = 1,   /* bad argument (null pointer, k/L out of range, dtype) */
+  GANN_EIO = 2,      /* a file could not be opened or is short */
+  GANN_EFORMAT = 3,  /* a file is malformed or inconsistent with the others */
+  GANN_ECUDA = 4,    /* a CUDA runtime call failed */
+  GANN_ENOMEM = 5,   /* device or host allocation failed */
+  GANN_EKERNEL = 6,  /* a kernel reported an error (bad id/degree, wait limit) */
+  GANN_ERANGE = 7    /* a size is beyond what this entry point supports */
+};
+
+/* element type of the base vectors; gustann::DataType, src/common.hpp:22-25 */
+enum { GANN_UINT8 = 0, GANN_FLOAT = 1 };
+
+/* gann_open flags */
+enum {
+  GANN_OPEN_NO_VALIDATE = 1 /* skip the load-time check of degrees and neighbour ids */
+};
+
+/* table precision for gann_search_batch */
+enum {
+  GANN_PREC_FP32 = 0,   /* FP32 tables built on CUDA cores */
+  GANN_PREC_BF16 = 1,   /* BF16 tensor-core table build (FP32 accumulate), BF16 table */
+  GANN_PREC_BF16X3 = 2  /* three-term split-BF16 tensor-core build, BF16 table */
+};
+
+typedef struct {
+  int64_t num_points;      /* Layout::num_data   src/layout.hpp:16 */
+  int64_t dim;             /* Layout::num_dims   src/layout.hpp:8  */
+  int64_t max_degree;      /* Layout::max_m0     src/layout.hpp:9  */
+  int64_t medoid;          /* Layout::enter_point src/layout.hpp:10 */
+  int64_t node_len;        /* Layout::node_size  src/layout.hpp:13 */
+  int64_t nodes_per_page;  /* Layout::nodes_per_page src/layout.hpp:18 */
+  int64_t num_pages;       /* Layout::num_pages  src/layout.hpp:15 */
+  int32_t pq_chunks;       /* PQSearchData::num_chunks src/pq_search.hpp:14 */
+  int32_t dtype;           /* GANN_UINT8 / GANN_FLOAT */
+  int32_t has_nav;         /* pivot graph loaded */
+  int32_t nav_points;      /* NavGraph::num_node src/nav_graph.hpp:12 */
+  int32_t nav_max_degree;  /* NavGraph::max_m src/nav_graph.hpp:14 */
+  int32_t device;          /* CUDA device the handle lives on */
+  int64_t device_bytes;    /* HBM held by the index */
+} gann_info_t;
+
+/*
+ * Open an index and make it resident in HBM.
+ * Replaces gustann::GustANN::GustANN(DataType) + GustANN::init_pure_mem(config,
+ * use_gpu_mem = true): src/ssd_search.hpp:70,76, src/ssd_search.cu:55-79,108-112,
+ * src/pure_mem.cu:27-69. Files: index_file is DiskANN's `_disk.index`
+ * (src/layout.cpp:11-69); `<pq_prefix>_pivots.bin` and `<pq_prefix>_compressed.bin`
+ * (src/ssd_search.cu:61-63, src/pq_search.cu:56-121); `<nav_dir>/nav_index`,
+ * `nav_index.data`, `map.txt` (src/ssd_search.cu:72-75, src/nav_graph.cu:41-100).
+ * nav_dir NULL or "" means "enter at the medoid" (src/pure_mem.cu:121-123).
+ */
+int gann_open(const char* index_file, const char* pq_prefix, const char* nav_dir, int dtype,
+              int flags, gann_t** out);
+
+/* Release the handle and its device memory. Replaces gustann::GustANN::~GustANN,
+ * src/ssd_search.cu:29-53. NULL is accepted. */
+int gann_close(gann_t* h);
+
+/* Describe an open index. The reference keeps these in gustann::Layout
+ * (src/layout.hpp:9-27); it has no accessor. */
+int gann_get_info(const gann_t* h, gann_info_t* out);
+
+/*
+ * Plain search (the drop-in form): FP32 tables, the reference's summation
+ * order and tie rules, ids identical to the reference's.
+ * Replaces gustann::GustANN::search, src/ssd_search.hpp:78-80 ->
+ * PureMemExecutor::search, src/pure_mem.cu:71-199. Host buffers:
+ * queries nq x dim float (uint8 queries converted to float, bin/search_disk.cpp:160-165),
+ * nns / distances nq x topk, found_cnt nq. Distances are squared L2. Unfilled
+ * slots hold id 0 and distance 0. run_time (may be NULL) receives the device
+ * time of entry selection + walk in seconds, the span the reference times
+ * (src/pure_mem.cu:101-187). topk and ef_search are >= 1 (the reference's
+ * driver also asserts ef_search >= topk, bin/search_disk.cpp:189-192; the
+ * library itself, like this one, accepts either order).
+ */
+int gann_search(gann_t* h, const float* queries, int nq, int topk, int ef_search, int32_t* nns,
+                float* distances, int32_t* found_cnt, double* run_time);
+
+/* Same as gann_search on device pointers, enqueued on `stream` (a cudaStream_t;
+ * NULL = the handle's stream) without a host synchronisation. The reference
+ * has no device-pointer form; this is PureMemExecutor::search (src/pure_mem.cu:71-199)
+ * minus its host<->device copies. */
+int gann_search_device(gann_t* h, const float* d_queries, int nq, int topk, int ef_search,
+                       int32_t* d_nns, float* d_distances, int32_t* d_found_cnt, void* stream);
+
+/* Synchronise `stream` (NULL = the handle's stream) and report, as
+ * GANN_EKERNEL, any error word left by kernels enqueued with
+ * gann_search_device; the word is cleared. The reference has no counterpart
+ * (its kernels report through device assert, src/impl/pure_mem.cuh:373). */
+int gann_check(gann_t* h, void* stream);
+
+/* FMA behaviour of the plain form at the reference's two contraction sites:
+ * the table accumulate (src/impl/pq.cuh:40) and the exact-distance accumulate
+ * (src/impl/util.cuh:37). Default 1/1 (fused), which tests/golden pins against
+ * the reference's own build. No counterpart in the reference (a compiler flag there). */
+int gann_set_fma(gann_t* h, int fma_table, int fma_exact);
+
+/* Pivot-graph sample (index preparation): the ids 0..num_data-1 shuffled with
+ * std::shuffle and std::mt19937(seed), the first num_samp kept and sorted.
+ * Replaces bin/gen_small_file.cpp:12-25 (seed 114514 there). */
+int gann_sample_pivots(int64_t num_data, int64_t num_samp, uint32_t seed, int32_t* out);
+
+/* Message for the last failing call on this thread. */
+const char* gann_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GANN_H_ */

@@ -1,0 +1,174 @@
+"""ctypes wrapper of the CPU oracle (oracle/_build/liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: used by tests/, __graft_entry__.smoke() and bench.py's
+CPU-baseline / reference legs as the checker and the timed CPU baseline. The
+product (gustann_b200) never imports it.
+"""
+from __future__ import annotations
+
+import ctypes
+import subprocess
+import time
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "_build" / "liboracle.so"
+REF_LIB = HERE / "_ref" / "libgustann_ref.so"
+
+FLAG_REF_UNDEFINED, FLAG_KEY_COLLISION, FLAG_BAD_ID, FLAG_BAD_DEG, FLAG_HOP_CAP, FLAG_NAV_CAP = 1, 2, 4, 8, 16, 32
+
+_lib = None
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+        L = ctypes.CDLL(str(LIB))
+        L.orc_open.restype = _I
+        L.orc_open.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, _I, ctypes.POINTER(_P)]
+        L.orc_close.argtypes = [_P]
+        L.orc_last_error.restype = ctypes.c_char_p
+        L.orc_info.argtypes = [_P, _P]
+        L.orc_exact_dist.restype = ctypes.c_float
+        L.orc_exact_dist.argtypes = [_P, _P, _I, _I, _I]
+        L.orc_pq_table.argtypes = [_P, _P, _I, _P, _P]
+        L.orc_nav_entry.restype = _I
+        L.orc_nav_entry.argtypes = [_P, _P, _I, _P]
+        L.orc_search_one.restype = _I
+        L.orc_search_one.argtypes = [_P, _P, _I, _I, _I, _I, _P, _P, _P, _P, _I, _P, _P, _P]
+        L.orc_search.restype = _I
+        L.orc_search.argtypes = [_P, _P, _I, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _P]
+        L.orc_max_threads.restype = _I
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+class Oracle:
+    """CPU restatement of the reference search (see gann_oracle.c)."""
+
+    def __init__(self, index_file: str, pq_prefix: str, nav_dir: str | None, dtype: int,
+                 fma_table: bool = True, fma_exact: bool = True):
+        self.h = _P()
+        rc = lib().orc_open(index_file.encode(), pq_prefix.encode(), nav_dir.encode() if nav_dir else None,
+                            dtype, ctypes.byref(self.h))
+        if rc:
+            raise RuntimeError(lib().orc_last_error().decode())
+        info = np.zeros(12, np.int64)
+        lib().orc_info(self.h, _p(info))
+        (self.n, self.dim, self.medoid, self.node_len, self.npp, self.max_m0, self.num_pages, self.M,
+         self.has_nav, self.nav_n, self.nav_max_m, self.nav_start) = (int(v) for v in info)
+        self.dtype = dtype
+        self.fma_table = int(fma_table)
+        self.fma_exact = int(fma_exact)
+
+    def close(self):
+        if self.h:
+            lib().orc_close(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def search(self, q: np.ndarray, k: int, L: int, threads: int = 0):
+        """Returns (ids, dists, found, hops, flags, entries) and sets self.last_seconds."""
+        q = np.ascontiguousarray(q, dtype=np.float32)
+        nq = q.shape[0]
+        ids = np.zeros((nq, k), np.int32)
+        dis = np.zeros((nq, k), np.float32)
+        fnd = np.zeros(nq, np.int32)
+        hops = np.zeros(nq, np.int32)
+        flags = np.zeros(nq, np.int32)
+        ent = np.zeros(nq, np.int32)
+        t0 = time.perf_counter()
+        rc = lib().orc_search(self.h, _p(q), nq, k, L, self.fma_table, self.fma_exact, threads, _p(ids), _p(dis),
+                              _p(fnd), _p(hops), _p(flags), _p(ent))
+        self.last_seconds = time.perf_counter() - t0
+        if rc and not flags.any():
+            raise RuntimeError(lib().orc_last_error().decode())
+        return ids, dis, fnd, hops, flags, ent
+
+    def search_one(self, q: np.ndarray, k: int, L: int, trace_cap: int = 100000):
+        q = np.ascontiguousarray(q, dtype=np.float32).reshape(-1)
+        ids = np.zeros(k, np.int32)
+        dis = np.zeros(k, np.float32)
+        fnd = np.zeros(1, np.int32)
+        trace = np.zeros(trace_cap, np.int32)
+        hops = np.zeros(1, np.int32)
+        flags = np.zeros(1, np.int32)
+        ent = np.zeros(1, np.int32)
+        lib().orc_search_one(self.h, _p(q), k, L, self.fma_table, self.fma_exact, _p(ids), _p(dis), _p(fnd),
+                             _p(trace), trace_cap, _p(hops), _p(flags), _p(ent))
+        return ids, dis, int(fnd[0]), trace[: min(int(hops[0]), trace_cap)], int(flags[0]), int(ent[0])
+
+    def pq_table(self, q: np.ndarray):
+        q = np.ascontiguousarray(q, dtype=np.float32).reshape(-1)
+        t = np.zeros((self.M, 256), np.float32)
+        qr = np.zeros(self.dim, np.float32)
+        lib().orc_pq_table(self.h, _p(q), self.fma_table, _p(t), _p(qr))
+        return t, qr
+
+    def nav_entry(self, q: np.ndarray) -> tuple[int, int]:
+        q = np.ascontiguousarray(q, dtype=np.float32).reshape(-1)
+        flags = np.zeros(1, np.int32)
+        local = lib().orc_nav_entry(self.h, _p(q), self.fma_exact, _p(flags))
+        return local, int(flags[0])
+
+
+def exact_dist(q: np.ndarray, v: np.ndarray, fma: bool = True) -> float:
+    q = np.ascontiguousarray(q, dtype=np.float32)
+    v = np.ascontiguousarray(v)
+    dtype = 0 if v.dtype == np.uint8 else 1
+    return float(lib().orc_exact_dist(_p(q), _p(v), dtype, q.shape[0], int(fma)))
+
+
+def max_threads() -> int:
+    return int(lib().orc_max_threads())
+
+
+class Reference:
+    """The reference's own search path built from its sources (oracle/build_ref.sh).
+    Needs a GPU; used only to pin the oracle and the product."""
+
+    def __init__(self, index_file: str, pq_prefix: str, nav_dir: str | None, dtype: int):
+        if not REF_LIB.exists():
+            raise FileNotFoundError(f"{REF_LIB} not built")
+        L = ctypes.CDLL(str(REF_LIB))
+        L.gref_open.restype = _P
+        L.gref_open.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, _I]
+        L.gref_search.restype = _I
+        L.gref_search.argtypes = [_P, _P, _I, _I, _I, _P, _P, _P, ctypes.POINTER(ctypes.c_double)]
+        L.gref_close.argtypes = [_P]
+        self.L = L
+        self.h = L.gref_open(index_file.encode(), pq_prefix.encode(), (nav_dir or "").encode(), dtype)
+        if not self.h:
+            raise RuntimeError("reference init_pure_mem failed")
+
+    def search(self, q: np.ndarray, k: int, L: int):
+        q = np.ascontiguousarray(q, dtype=np.float32)
+        nq = q.shape[0]
+        ids = np.zeros((nq, k), np.int32)
+        dis = np.zeros((nq, k), np.float32)
+        fnd = np.zeros(nq, np.int32)
+        t = ctypes.c_double(0.0)
+        rc = self.L.gref_search(self.h, _p(q), nq, k, L, _p(ids), _p(dis), _p(fnd), ctypes.byref(t))
+        if rc:
+            raise RuntimeError("reference search failed")
+        return ids, dis, fnd, t.value
+
+    def close(self):
+        if self.h:
+            self.L.gref_close(self.h)
+            self.h = None
