@@ -1,0 +1,499 @@
+"""Benchmark of the B200 GustANN all-in-GPU search path.
+
+One step = one search of the whole query batch (default 10,000 queries) on the
+index of the chosen workload, at the smallest L whose recall@10 reaches the
+target (0.95). Prints one JSON line.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload c0|c1|c2|small] [--form plain]
+
+Multi-GPU (torchrun, one process per GPU): every rank holds a replica of the
+index and searches its own full query batch (weak scaling, no collective on the
+data path); the reported value is all ranks' queries / the slowest rank's time.
+
+--impl reference runs the reference algorithm on the host cores: the CPU
+restatement in oracle/ (bit-exact with the reference's kernel on the committed
+fixtures), over all host threads, one bounded sample of the queries per step.
+When the reference's own CUDA build (oracle/_ref) is present it is timed too and
+reported beside it.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "QPS@recall@10=0.95 on 1 B200 (batched/BF16 vs plain GPU); p50/p99 ms under load"
+WORKLOADS = {
+    # name: kind, n, dim, clusters, R, M, nav samples
+    "small": ("u8", 100_000, 128, 100, 64, 32, 1_000),
+    "c0": ("u8", 1_000_000, 128, 1_000, 64, 32, 10_000),
+    "c1": ("f32", 10_000_000, 96, 4_096, 64, 32, 100_000),
+    "c2": ("u8", 100_000_000, 128, 10_000, 32, 32, 1_000_000),
+}
+L_LADDER = [16, 24, 32, 48, 64, 96, 128, 160, 192, 256, 320, 384, 448, 512, 640, 768, 1024, 1536, 2048]
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ----------------------------------------------------------------------------- distributed plumbing
+
+def dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), \
+        int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def init_dist(world: int, backend: str):
+    import datetime
+
+    import torch.distributed as dist
+
+    if world > 1 and not dist.is_initialized():
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return dist
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(x: float, world: int, device=None) -> float:
+    """Max of a float over ranks (all_reduce MAX); identity for one rank."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def wait_for(path: Path, seconds: float) -> None:
+    t0 = time.time()
+    while not path.exists():
+        if time.time() - t0 > seconds:
+            raise TimeoutError(f"{path} did not appear within {seconds} s")
+        time.sleep(2.0)
+
+
+# ----------------------------------------------------------------------------- workload preparation
+
+def prepare(workload: str, nq: int, cache: Path, rank_local: int) -> dict:
+    """Build (once per box) the index, queries and ground truth of a workload."""
+    kind, n, dim, clusters, R, M, nav = WORKLOADS[workload]
+    d = cache / f"{workload}_nq{nq}"
+    ready = d / "ready.json"
+    if not ready.exists():
+        if rank_local == 0:
+            import torch
+
+            from gustann_b200.indexing import build_index, groundtruth, synth
+
+            d.mkdir(parents=True, exist_ok=True)
+            t0 = time.time()
+            base, qs = synth.make(kind, n, dim, clusters, nq, backend="torch", device="cuda")
+            f = build_index(base, str(d), R=R, M=M, nav_samples=nav, device="cuda")
+            gt = groundtruth.knn(base, qs, 100)
+            np.save(d / "queries.npy", qs.float().cpu().numpy())
+            np.save(d / "gt.npy", gt)
+            meta = {"workload": workload, "kind": kind, "n": n, "dim": dim, "clusters": clusters, "R": R, "M": M,
+                    "nav": nav, "nq": nq, "index_file": f.index_file, "pq_prefix": f.pq_prefix,
+                    "nav_dir": f.nav_dir, "build_s": time.time() - t0, "timings": f.timings}
+            del base
+            torch.cuda.empty_cache()
+            ready.write_text(json.dumps(meta))
+        else:
+            wait_for(ready, 3600)
+    meta = json.loads(ready.read_text())
+    meta["queries"] = np.load(d / "queries.npy")
+    meta["gt"] = np.load(d / "gt.npy")
+    return meta
+
+
+# ----------------------------------------------------------------------------- clocks
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        import torch
+
+        try:
+            self.gpu = "GPU-" + str(torch.cuda.get_device_properties(device).uuid)
+        except Exception:
+            self.gpu = str(device)
+        self.proc = None
+        self.path = Path(tempfile.mkstemp(prefix="gann_clocks_", suffix=".csv")[1])
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in self.path.read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        self.path.unlink(missing_ok=True)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ----------------------------------------------------------------------------- our arm
+
+def recall_at(ids: np.ndarray, gt: np.ndarray, k: int) -> float:
+    from gustann_b200.indexing.groundtruth import recall
+
+    return recall(ids, gt, k)
+
+
+class PlainRunner:
+    """gann_search_device_ex on resident device buffers (the `value` path)."""
+
+    def __init__(self, g, q_dev, k):
+        import torch
+
+        self.g, self.q, self.k = g, q_dev, k
+        nq = q_dev.shape[0]
+        self.nq = nq
+        self.ids = torch.zeros((nq, k), dtype=torch.int32, device="cuda")
+        self.dis = torch.zeros((nq, k), dtype=torch.float32, device="cuda")
+        self.fnd = torch.zeros(nq, dtype=torch.int32, device="cuda")
+        self.hops = torch.zeros(nq, dtype=torch.int32, device="cuda")
+        self.bytes = torch.zeros(nq, dtype=torch.int64, device="cuda")
+
+    def run(self, L, counters=False):
+        import torch
+
+        s = torch.cuda.current_stream().cuda_stream
+        self.g.search_device_ex(self.q.data_ptr(), self.nq, self.k, L, self.ids.data_ptr(), self.dis.data_ptr(),
+                                self.fnd.data_ptr(), self.hops.data_ptr() if counters else 0,
+                                self.bytes.data_ptr() if counters else 0, s)
+
+    launches_per_step = 1
+
+
+def calibrate(runner, gt, k, target, fixed_L=None):
+    import torch
+
+    ladder = [fixed_L] if fixed_L else L_LADDER
+    best = None
+    for L in ladder:
+        if L < k:
+            continue
+        runner.run(L)
+        torch.cuda.synchronize()
+        runner.g.check()
+        r = recall_at(runner.ids.cpu().numpy(), gt, k)
+        best = (L, r)
+        if r >= target:
+            break
+    return best
+
+
+def time_steps(runner, L, steps, warmup, world, flush):
+    import torch
+
+    for _ in range(warmup):
+        flush.zero_()
+        runner.run(L)
+    torch.cuda.synchronize()
+    barrier(world)
+    times = []
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    torch.cuda.synchronize()
+    for i in range(steps):
+        flush.zero_()  # evict L2 (buffer larger than the 126 MB L2) outside the timed span
+        ev[i][0].record()
+        runner.run(L)
+        ev[i][1].record()
+    torch.cuda.synchronize()
+    barrier(world)
+    runner.g.check()
+    times = [a.elapsed_time(b) for a, b in ev]
+    return times
+
+
+def e2e_steps(g, q_host_pinned, k, L, steps, warmup):
+    """Public host-buffer API (gann_search): H2D of the queries and D2H of the
+    results inside every step."""
+    nq = q_host_pinned.shape[0]
+    import torch
+
+    ids = torch.zeros((nq, k), dtype=torch.int32).pin_memory()
+    dis = torch.zeros((nq, k), dtype=torch.float32).pin_memory()
+    fnd = torch.zeros(nq, dtype=torch.int32).pin_memory()
+    import ctypes
+
+    import gustann_b200 as gb
+
+    t = ctypes.c_double()
+
+    def one():
+        rc = gb.lib().gann_search(g.handle, q_host_pinned.data_ptr(), nq, k, L, ids.data_ptr(), dis.data_ptr(),
+                                  fnd.data_ptr(), ctypes.byref(t))
+        gb._check(rc)
+
+    for _ in range(warmup):
+        one()
+    ts = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        one()
+        ts.append(time.perf_counter() - t0)
+    h2d = nq * q_host_pinned.shape[1] * 4
+    d2h = nq * k * 8 + nq * 4
+    return nq / float(np.mean(ts)), h2d, d2h
+
+
+def cpu_baseline(meta, L, k, budget_s=15.0):
+    """The oracle (CPU restatement of the reference path) on all host cores, on a
+    bounded sample of the same queries."""
+    from oracle.oracle import Oracle, max_threads
+
+    dtype = 0 if meta["kind"] == "u8" else 1
+    o = Oracle(meta["index_file"], meta["pq_prefix"], meta["nav_dir"], dtype)
+    q = meta["queries"]
+    cores = max_threads()
+    probe = min(len(q), max(64, cores * 8))
+    o.search(q[:probe], k, L, threads=cores)
+    rate = probe / max(o.last_seconds, 1e-6)
+    sample = int(min(len(q), max(probe, rate * budget_s)))
+    ids, *_ = o.search(q[:sample], k, L, threads=cores)
+    val = sample / o.last_seconds
+    o.close()
+    return {"value": val, "unit": "queries/s", "cores": cores, "kind": "port",
+            "sample": f"first {sample} of the {len(q)} queries, k={k}, L={L}, {o.last_seconds:.1f} s, "
+                      f"{cores} threads (oracle/gann_oracle.c)"}, ids
+
+
+def load_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d.get("hbm_gbs"), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_per_query(kernel: str, workload: str):
+    """DRAM bytes per query of `kernel` from a committed ncu summary, if any."""
+    p = ROOT / "profiles" / f"{kernel}_{workload}.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d.get("dram_bytes_per_query")
+    return None
+
+
+def run_ours(args, rank, world, local):
+    import torch
+
+    import gustann_b200 as gb
+
+    torch.cuda.set_device(local)
+    init_dist(world, "nccl")
+    cache = Path(args.cache)
+    meta = prepare(args.workload, args.nq, cache, local)
+    barrier(world)
+    dtype = gb.DataType.UINT8 if meta["kind"] == "u8" else gb.DataType.FLOAT
+    g = gb.GustANN(dtype)
+    g.init_pure_mem(gb.GustANNConfig(meta["index_file"], meta["pq_prefix"], meta["nav_dir"] or ""))
+    q = torch.from_numpy(meta["queries"]).cuda()
+    gt = meta["gt"]
+    k = args.k
+    runner = PlainRunner(g, q, k)
+    L, rec = calibrate(runner, gt, k, args.recall, args.L)
+    # device counters: hops and algorithmic bytes of one step (same work every step)
+    runner.run(L, counters=True)
+    torch.cuda.synchronize()
+    hops = runner.hops.cpu().numpy()
+    step_bytes = int(runner.bytes.sum().item())
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    clocks = ClockSampler(local)
+    clocks.start()
+    times_ms = time_steps(runner, L, args.steps, args.warmup, world, flush)
+    clk = clocks.stop()
+    total_ms = max_over_ranks(float(sum(times_ms)), world, device="cuda")
+    nq = runner.nq
+    value = world * nq * args.steps / (total_ms / 1e3)
+    avg_ms = float(np.mean(times_ms))
+    peak, peak_kind = load_peaks()
+    achieved = step_bytes / (avg_ms / 1e3) / 1e9
+    tpq = traffic_per_query("plain_search_kernel", args.workload)
+    # end to end through the public host API
+    qp = torch.from_numpy(meta["queries"]).pin_memory()
+    e2e_val, h2d, d2h = e2e_steps(g, qp, k, L, max(2, min(args.steps, 5)), 1)
+    e2e_total = max_over_ranks(1.0 / e2e_val, world, device="cuda")
+    out = {
+        "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": f"synthetic seeded Gaussian mixture ({meta['clusters']} clusters) standing in for "
+                f"{'SIFT' if meta['kind'] == 'u8' else 'DEEP'}; index built on the device",
+        "config": {"workload": args.workload, "n": meta["n"], "dim": meta["dim"], "vector": meta["kind"],
+                   "R": meta["R"], "pq_chunks": meta["M"], "nav_points": meta["nav"], "queries_per_step": nq,
+                   "k": k, "L": L, "form": "plain", "l2": "flushed (256 MB write) before every step",
+                   "parallelism": f"replicas x{world}"},
+        "recall": rec, "recall_target": args.recall,
+        "hops_per_query": float(hops.mean()),
+        "gathered_bytes_per_query": step_bytes / nq,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak if peak else None,
+                     "traffic": None if tpq is None else tpq * nq, "peak_kind": peak_kind,
+                     "kernel": "plain_search_kernel"},
+        "e2e": {"value": world / e2e_total, "unit": "queries/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": runner.launches_per_step * args.steps,
+        "clocks": clk,
+        "build_s": meta.get("build_s"),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        out["cpu_baseline"], _ = cpu_baseline(meta, L, k, args.cpu_budget)
+    g.close()
+    barrier(world)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+# ----------------------------------------------------------------------------- reference arm
+
+def run_reference(args, rank, world, local):
+    if rank != 0:
+        return
+    import torch
+
+    from oracle.oracle import REF_LIB, Oracle, Reference, max_threads
+
+    torch.cuda.set_device(local)
+    meta = prepare(args.workload, args.nq, Path(args.cache), local)
+    dtype = 0 if meta["kind"] == "u8" else 1
+    k = args.k
+    q, gt = meta["queries"], meta["gt"]
+    o = Oracle(meta["index_file"], meta["pq_prefix"], meta["nav_dir"], dtype)
+    cores = max_threads()
+    # L for the recall target, with the reference algorithm itself (on a subsample)
+    sub = min(len(q), 1000)
+    L = args.L
+    if not L:
+        for L in L_LADDER:
+            if L < k:
+                continue
+            ids, *_ = o.search(q[:sub], k, L, threads=cores)
+            if recall_at(ids, gt[:sub], k) >= args.recall:
+                break
+    probe = min(len(q), max(64, cores * 8))
+    o.search(q[:probe], k, L, threads=cores)
+    rate = probe / max(o.last_seconds, 1e-6)
+    total_budget = 120.0
+    per_step = total_budget / max(1, args.steps + args.warmup)
+    sample = int(min(len(q), max(probe, rate * per_step)))
+    for _ in range(args.warmup):
+        o.search(q[:sample], k, L, threads=cores)
+    secs = []
+    for _ in range(args.steps):
+        ids, *_ = o.search(q[:sample], k, L, threads=cores)
+        secs.append(o.last_seconds)
+    value = sample * args.steps / sum(secs)
+    rec = recall_at(ids, gt[:sample], k)
+    out = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(secs) / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic seeded Gaussian mixture; same index files as the GPU arm",
+        "config": {"workload": args.workload, "n": meta["n"], "dim": meta["dim"], "vector": meta["kind"],
+                   "R": meta["R"], "pq_chunks": meta["M"], "queries_per_step": sample, "k": k, "L": L,
+                   "form": "reference algorithm on host cores"},
+        "recall": rec,
+        "cpu_baseline": {"value": value, "unit": "queries/s", "cores": cores, "kind": "port",
+                         "sample": f"first {sample} of {len(q)} queries per step, k={k}, L={L}, "
+                                   f"{cores} threads, oracle/gann_oracle.c (bit-exact with the reference "
+                                   f"kernel on the committed fixtures)"},
+        "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    o.close()
+    if REF_LIB.exists() and not args.no_ref_gpu:
+        # The reference's own -G path built from its sources, timed by its own
+        # timer (nav + host translate + walk, src/pure_mem.cu:101-187).
+        try:
+            r = Reference(meta["index_file"], meta["pq_prefix"], meta["nav_dir"], dtype)
+            r.search(q, k, L)
+            ts = []
+            for _ in range(3):
+                ids, dis, fnd, t = r.search(q, k, L)
+                ts.append(t)
+            out["reference_cuda_kernel"] = {
+                "value": len(q) / float(np.median(ts)), "unit": "queries/s", "L": L, "queries": len(q),
+                "recall": recall_at(ids, gt, k),
+                "note": "reference search_graph_kernel_gpumem + nav kernel compiled for sm_100a from its "
+                        "sources (oracle/build_ref.sh), its own wall-clock timer, median of 3"}
+            r.close()
+        except Exception as e:  # reported, not fatal
+            out["reference_cuda_kernel"] = {"error": str(e)}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=list(WORKLOADS), default="c0")
+    ap.add_argument("--nq", type=int, default=10_000)
+    ap.add_argument("--k", type=int, default=10)
+    ap.add_argument("--recall", type=float, default=0.95)
+    ap.add_argument("--L", type=int, default=0, help="fixed L (skip calibration)")
+    ap.add_argument("--cache", default=os.environ.get("GANN_BENCH_CACHE", "/tmp/gann_bench"))
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-ref-gpu", action="store_true")
+    args = ap.parse_args()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank, world, local)
+    else:
+        run_ours(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -75,6 +75,7 @@ _SIGNATURES = {
     "gann_get_info": (_I, [_P, ctypes.POINTER(GannInfo)]),
     "gann_search": (_I, [_P, _P, _I, _I, _I, _P, _P, _P, ctypes.POINTER(ctypes.c_double)]),
     "gann_search_device": (_I, [_P, _P, _I, _I, _I, _P, _P, _P, _P]),
+    "gann_search_device_ex": (_I, [_P, _P, _I, _I, _I, _P, _P, _P, _P, _P, _P]),
     "gann_check": (_I, [_P, _P]),
     "gann_set_fma": (_I, [_P, _I, _I]),
     "gann_last_error": (ctypes.c_char_p, []),
@@ -186,6 +187,12 @@ class GustANN:
         """Device-pointer form (gann_search_device); enqueued without a host sync."""
         _check(lib().gann_search_device(self.handle, d_q, nq, topk, ef_search, d_nns, d_dists, d_found,
                                         stream or None))
+
+    def search_device_ex(self, d_q: int, nq: int, topk: int, ef_search: int, d_nns: int, d_dists: int,
+                         d_found: int, d_hops: int = 0, d_bytes: int = 0, stream: int = 0) -> None:
+        """gann_search_device_ex: also writes per-query hop and gathered-byte counters."""
+        _check(lib().gann_search_device_ex(self.handle, d_q, nq, topk, ef_search, d_nns, d_dists, d_found,
+                                           d_hops or None, d_bytes or None, stream or None))
 
     def check(self, stream: int = 0) -> None:
         _check(lib().gann_check(self.handle, stream or None))

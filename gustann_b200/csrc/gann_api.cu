@@ -168,6 +168,7 @@ gann::PlainParams make_params(gann_index* h, const float* d_q, int nq, int topk,
   p.dists = d_dists;
   p.found = d_found;
   p.hops = nullptr;
+  p.bytes = nullptr;
   p.next_query = h->d_counter;
   p.err = h->d_err;
   return p;
@@ -296,8 +297,9 @@ int gann_get_info(const gann_t* h, gann_info_t* out) {
   return GANN_OK;
 }
 
-int gann_search_device(gann_t* h, const float* d_queries, int nq, int topk, int ef_search, int32_t* d_nns,
-                       float* d_distances, int32_t* d_found_cnt, void* stream) {
+int gann_search_device_ex(gann_t* h, const float* d_queries, int nq, int topk, int ef_search, int32_t* d_nns,
+                          float* d_distances, int32_t* d_found_cnt, int32_t* d_hops, int64_t* d_bytes,
+                          void* stream) {
   int rc = check_search_args(h, nq, topk, ef_search);
   if (rc) return rc;
   if (nq == 0) return GANN_OK;
@@ -305,10 +307,18 @@ int gann_search_device(gann_t* h, const float* d_queries, int nq, int topk, int 
   std::lock_guard<std::mutex> lk(h->mu);
   cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
   gann::PlainParams p = make_params(h, d_queries, nq, topk, ef_search, d_nns, d_distances, d_found_cnt);
+  p.hops = d_hops;
+  p.bytes = d_bytes;
   cudaError_t e = cudaMemsetAsync(h->d_counter, 0, sizeof(int), s);
   if (e == cudaSuccess) e = gann::launch_plain(p, h->hx.dtype, h->num_sms, s);
   if (e != cudaSuccess) return set_error(GANN_ECUDA, std::string("plain search launch: ") + cudaGetErrorString(e));
   return GANN_OK;
+}
+
+int gann_search_device(gann_t* h, const float* d_queries, int nq, int topk, int ef_search, int32_t* d_nns,
+                       float* d_distances, int32_t* d_found_cnt, void* stream) {
+  return gann_search_device_ex(h, d_queries, nq, topk, ef_search, d_nns, d_distances, d_found_cnt, nullptr,
+                               nullptr, stream);
 }
 
 int gann_search(gann_t* h, const float* queries, int nq, int topk, int ef_search, int32_t* nns, float* distances,

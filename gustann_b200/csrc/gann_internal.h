@@ -67,7 +67,8 @@ struct PlainParams {
   int32_t* nns;              // nq x k
   float* dists;              // nq x k
   int32_t* found;            // nq
-  int32_t* hops;             // nq or null
+  int32_t* hops;             // nq or null: hops (expanded nodes) per query
+  int64_t* bytes;            // nq or null: algorithmic gathered bytes per query
   int* next_query;           // work counter, zeroed before launch
   unsigned int* err;         // error word
 };

@@ -109,11 +109,13 @@ __device__ WarpSmem carve(uint8_t* base, int M, int L, int max_m, int k, int dim
 // get_entry_kernel_inner (nav.cuh:13-135) for one query, one slot per lane.
 // Returns the pivot graph's local id, or -1 after setting an error bit.
 template <class T>
-__device__ int nav_entry(const PlainParams& p, const float* q, int lane) {
+__device__ int nav_entry(const PlainParams& p, const float* q, int lane, int64_t& gathered) {
   const T* nd = reinterpret_cast<const T*>(p.ix.nav_data);
   const int dim = p.dim;
   const int64_t glen = (int64_t)p.nav_n * p.nav_max_m;
   float d0 = warp_exact<T>(q, nd + (size_t)p.nav_start * dim, dim, lane, p.fma_exact);
+  const int vec_bytes = dim * (int)sizeof(T);
+  gathered += vec_bytes;
   uint32_t my_id = lane == 0 ? (uint32_t)p.nav_start : 0xffffffffu;  // nav.cuh:50-57
   float my_d = lane == 0 ? d0 : inf_f();
   int idx = 0, iters = 0;
@@ -132,6 +134,8 @@ __device__ int nav_entry(const PlainParams& p, const float* q, int lane) {
     }
     unsigned neg = __ballot_sync(kFull, lane < kNavR && v == -1);
     int deg = neg ? __ffs(neg) - 1 : kNavR;
+    // row slots read up to and including the first -1, plus one vector per neighbour
+    gathered += 4 * (deg < kNavR ? deg + 1 : kNavR) + (int64_t)deg * vec_bytes;
     for (int i = 0; i < deg; i++) {  // nav.cuh:70-81
       int vi = __shfl_sync(kFull, v, i);
       if ((unsigned)vi >= (unsigned)p.nav_n) {
@@ -286,8 +290,9 @@ __device__ void search_query(const PlainParams& p, const WarpSmem& s, int qid, i
   __syncwarp();
 
   int64_t u;
+  int64_t gathered = 0;  // algorithmic bytes: records, neighbour ids, codes, pivot vectors
   if (p.has_nav) {  // pure_mem.cu:106-124
-    int local = nav_entry<T>(p, s.q, lane);
+    int local = nav_entry<T>(p, s.q, lane, gathered);
     if (local >= p.nav_n) {  // an all-INF slot 0 (fewer than 4 finite candidates)
       if (lane == 0) atomicOr(p.err, kErrBadId);
       local = -1;
@@ -331,6 +336,7 @@ __device__ void search_query(const PlainParams& p, const WarpSmem& s, int qid, i
       if (lane == 0) atomicOr(p.err, kErrBadId);
       break;
     }
+    gathered += 4 + 4 * deg + p.data_len + (int64_t)deg * M;
     __syncwarp();
     // Sort the new entries by (dist, id) -- pure_mem.cuh:314-348 sorts them by
     // merge rounds; with distinct ids any correct sort gives the same order.
@@ -426,6 +432,7 @@ __device__ void search_query(const PlainParams& p, const WarpSmem& s, int qid, i
   if (lane == 0) {
     p.found[qid] = found;
     if (p.hops) p.hops[qid] = hops;
+    if (p.bytes) p.bytes[qid] = gathered;
   }
   __syncwarp();
 }

@@ -110,6 +110,14 @@ int gann_search(gann_t* h, const float* queries, int nq, int topk, int ef_search
 int gann_search_device(gann_t* h, const float* d_queries, int nq, int topk, int ef_search,
                        int32_t* d_nns, float* d_distances, int32_t* d_found_cnt, void* stream);
 
+/* gann_search_device plus per-query counters (device arrays of nq, each may be
+ * NULL): d_hops = nodes expanded, d_bytes = algorithmic gathered bytes (degree
+ * word, neighbour ids, vector and the codes of every scored neighbour per hop,
+ * plus the pivot-graph rows and vectors). No counterpart in the reference. */
+int gann_search_device_ex(gann_t* h, const float* d_queries, int nq, int topk, int ef_search,
+                          int32_t* d_nns, float* d_distances, int32_t* d_found_cnt, int32_t* d_hops,
+                          int64_t* d_bytes, void* stream);
+
 /* Synchronise `stream` (NULL = the handle's stream) and report, as
  * GANN_EKERNEL, any error word left by kernels enqueued with
  * gann_search_device; the word is cleared. The reference has no counterpart
