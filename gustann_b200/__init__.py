@@ -113,6 +113,17 @@ def _ptr(a: np.ndarray) -> int:
     return a.ctypes.data
 
 
+_CUDA_STREAM_LEGACY = 1  # cudaStreamLegacy
+
+
+def _stream(stream):
+    """None -> NULL (the handle's stream); 0 (torch's legacy default stream) ->
+    cudaStreamLegacy; anything else is passed through."""
+    if stream is None:
+        return None
+    return _CUDA_STREAM_LEGACY if stream == 0 else stream
+
+
 def sample_pivots(num_data: int, num_samp: int, seed: int = 114514) -> np.ndarray:
     """The pivot-graph sample of bin/gen_small_file.cpp:12-25 (sorted global ids)."""
     out = np.empty(num_samp, dtype=np.int32)
@@ -183,19 +194,21 @@ class GustANN:
         return nns, dis, fnd, st.run_time
 
     def search_device(self, d_q: int, nq: int, topk: int, ef_search: int, d_nns: int, d_dists: int,
-                      d_found: int, stream: int = 0) -> None:
-        """Device-pointer form (gann_search_device); enqueued without a host sync."""
+                      d_found: int, stream: int | None = None) -> None:
+        """Device-pointer form (gann_search_device); enqueued without a host sync.
+        ``stream``: a cudaStream_t value (0 = the legacy default stream, as torch
+        reports it), or None for the handle's own stream."""
         _check(lib().gann_search_device(self.handle, d_q, nq, topk, ef_search, d_nns, d_dists, d_found,
-                                        stream or None))
+                                        _stream(stream)))
 
     def search_device_ex(self, d_q: int, nq: int, topk: int, ef_search: int, d_nns: int, d_dists: int,
-                         d_found: int, d_hops: int = 0, d_bytes: int = 0, stream: int = 0) -> None:
+                         d_found: int, d_hops: int = 0, d_bytes: int = 0, stream: int | None = None) -> None:
         """gann_search_device_ex: also writes per-query hop and gathered-byte counters."""
         _check(lib().gann_search_device_ex(self.handle, d_q, nq, topk, ef_search, d_nns, d_dists, d_found,
-                                           d_hops or None, d_bytes or None, stream or None))
+                                           d_hops or None, d_bytes or None, _stream(stream)))
 
-    def check(self, stream: int = 0) -> None:
-        _check(lib().gann_check(self.handle, stream or None))
+    def check(self, stream: int | None = None) -> None:
+        _check(lib().gann_check(self.handle, _stream(stream)))
 
     def close(self) -> None:
         if self._h is not None:

@@ -69,41 +69,62 @@ __device__ __forceinline__ int lower_bound_key(const float* dist, const uint32_t
 struct WarpSmem {
   float* table;       // M x 256
   float* q;           // dim: the query, then the restored query
-  uint32_t* list_id;  // L   sorted candidate list
-  float* list_d;
-  uint32_t* new_id;   // max_m  neighbours of the node being expanded
+  uint32_t* la_id;    // L   sorted candidate list (ping)
+  float* la_d;
+  uint32_t* lb_id;    // L   (pong)
+  float* lb_d;
+  uint32_t* new_id;   // max_m  neighbours of the node being expanded, then the survivors
   float* new_d;
-  uint32_t* snew_id;  // max_m  the same, sorted
-  float* snew_d;
-  uint32_t* mer_id;   // L + max_m  merged list
-  float* mer_d;
+  uint32_t* sv_id;    // max_m  surviving neighbours, sorted
+  float* sv_d;
+  int32_t* sv_lb;     // max_m  their insertion points in the old list
+  int32_t* sv_slb;    // max_m  insertion points in sorted order
   int32_t* topk_id;   // k
   float* topk_d;
 };
 
 __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 
+// Byte offsets of the arrays above inside one warp's slice (host and device).
+struct SmemPlan {
+  size_t off[14];
+  size_t total;
+  __host__ __device__ SmemPlan(int M, int L, int max_m, int k, int dim) {
+    const size_t sz[14] = {sizeof(float) * (size_t)M * kPivots, sizeof(float) * (size_t)dim, 4 * (size_t)L,
+                           4 * (size_t)L, 4 * (size_t)L, 4 * (size_t)L, 4 * (size_t)max_m, 4 * (size_t)max_m,
+                           4 * (size_t)max_m, 4 * (size_t)max_m, 4 * (size_t)max_m, 4 * (size_t)max_m,
+                           4 * (size_t)k, 4 * (size_t)k};
+    size_t o = 0;
+    for (int i = 0; i < 14; i++) {
+      off[i] = o;
+      o = align16(o + sz[i]);
+    }
+    total = o;
+  }
+};
+
 __device__ WarpSmem carve(uint8_t* base, int M, int L, int max_m, int k, int dim) {
+  const SmemPlan pl(M, L, max_m, k, dim);
   WarpSmem s;
-  size_t o = 0;
-  auto take = [&](size_t bytes) {
-    uint8_t* p = base + o;
-    o = align16(o + bytes);
-    return p;
-  };
-  s.table = (float*)take(sizeof(float) * (size_t)M * kPivots);
-  s.q = (float*)take(sizeof(float) * dim);
-  s.list_id = (uint32_t*)take(4 * (size_t)L);
-  s.list_d = (float*)take(4 * (size_t)L);
-  s.new_id = (uint32_t*)take(4 * (size_t)max_m);
-  s.new_d = (float*)take(4 * (size_t)max_m);
-  s.snew_id = (uint32_t*)take(4 * (size_t)max_m);
-  s.snew_d = (float*)take(4 * (size_t)max_m);
-  s.mer_id = (uint32_t*)take(4 * (size_t)(L + max_m));
-  s.mer_d = (float*)take(4 * (size_t)(L + max_m));
-  s.topk_id = (int32_t*)take(4 * (size_t)k);
-  s.topk_d = (float*)take(4 * (size_t)k);
+  s.table = (float*)(base + pl.off[0]);
+  s.q = (float*)(base + pl.off[1]);
+  s.la_id = (uint32_t*)(base + pl.off[2]);
+  s.la_d = (float*)(base + pl.off[3]);
+  s.lb_id = (uint32_t*)(base + pl.off[4]);
+  s.lb_d = (float*)(base + pl.off[5]);
+  s.new_id = (uint32_t*)(base + pl.off[6]);
+  s.new_d = (float*)(base + pl.off[7]);
+  s.sv_id = (uint32_t*)(base + pl.off[8]);
+  s.sv_d = (float*)(base + pl.off[9]);
+  s.sv_lb = (int32_t*)(base + pl.off[10]);
+  s.sv_slb = (int32_t*)(base + pl.off[11]);
+  s.topk_id = (int32_t*)(base + pl.off[12]);
+  s.topk_d = (float*)(base + pl.off[13]);
   return s;
+}
+
+__device__ __forceinline__ bool key_less(float a, uint32_t ai, float b, uint32_t bi) {
+  return a < b || (a == b && (ai & kMask) < (bi & kMask));
 }
 
 // get_entry_kernel_inner (nav.cuh:13-135) for one query, one slot per lane.
@@ -304,6 +325,10 @@ __device__ void search_query(const PlainParams& p, const WarpSmem& s, int qid, i
   build_table(p, s, lane);
 
   int sz = 0, found = 0, hops = 0;
+  uint32_t* list_id = s.la_id;
+  float* list_d = s.la_d;
+  uint32_t* out_id_l = s.lb_id;
+  float* out_d_l = s.lb_d;
   while (u >= 0) {  // pure_mem.cuh:287-428
     if (u >= p.n) {
       if (lane == 0) atomicOr(p.err, kErrBadId);
@@ -338,88 +363,119 @@ __device__ void search_query(const PlainParams& p, const WarpSmem& s, int qid, i
     }
     gathered += 4 + 4 * deg + p.data_len + (int64_t)deg * M;
     __syncwarp();
-    // Sort the new entries by (dist, id) -- pure_mem.cuh:314-348 sorts them by
-    // merge rounds; with distinct ids any correct sort gives the same order.
-    for (int t = lane; t < deg; t += 32) {
-      const float d = s.new_d[t];
-      const uint32_t id = s.new_id[t] & kMask;
-      int r = 0;
-      for (int f = 0; f < deg; f++) {
-        const float fd = s.new_d[f];
-        const uint32_t fi = s.new_id[f] & kMask;
-        r += (fd < d) || (fd == d && (fi < id || (fi == id && f < t)));
-      }
-      s.snew_d[r] = d;
-      s.snew_id[r] = s.new_id[t];
-    }
-    __syncwarp();
-    // Merge into the sorted list; a new entry equal to an old one goes after
-    // it (pure_mem.cuh:351-376); positions past 2L are dropped (:377).
-    const int cap2 = min(sz + deg, 2 * L);
-    for (int t = lane; t < deg; t += 32) {
-      const float d = s.snew_d[t];
-      const uint32_t id = s.snew_id[t];
-      int pos = lower_bound_key(s.list_d, s.list_id, 0, sz, d, id);
-      if (pos != sz && ((s.list_id[pos] ^ id) & kMask) == 0) pos++;
-      pos += t;
-      if (pos < cap2) {
-        s.mer_d[pos] = d;
-        s.mer_id[pos] = id;
-      }
-    }
-    for (int i = lane; i < sz; i += 32) {
-      const float d = s.list_d[i];
-      const uint32_t id = s.list_id[i];
-      int pos = lower_bound_key(s.snew_d, s.snew_id, 0, deg, d, id) + i;
-      if (pos < cap2) {
-        s.mer_d[pos] = d;
-        s.mer_id[pos] = id;
-      }
-    }
-    __syncwarp();
-    // Drop adjacent duplicate ids, keep at most L entries and find the first
-    // entry without the expanded bit (pure_mem.cuh:380-419).
-    int count = 0, best = INT_MAX;
-    for (int base = 0; base < cap2; base += 32) {
-      const int i = base + lane;
-      const bool valid = i < cap2;
-      uint32_t id = 0;
+    // Merge the new entries into the sorted list. The reference merges all of
+    // them (pure_mem.cuh:314-376), cuts the result at 2L (:377), drops ids equal
+    // to their predecessor (a new copy always lands right after the old one,
+    // :358-360) and keeps L entries (:416). The same list results from
+    // inserting only the survivors: entries whose id is not in the list yet and
+    // whose key (dist, id) is below the list's last key when the list is full.
+    const bool full = sz == L;
+    const float tail_d = full ? list_d[L - 1] : 0.0f;
+    const uint32_t tail_id = full ? list_id[L - 1] : 0u;
+    int nsv = 0;
+    for (int base = 0; base < deg; base += 32) {
+      const int t = base + lane;
+      bool keep = false;
       float d = 0.0f;
-      bool dup = false;
-      if (valid) {
-        id = s.mer_id[i];
-        d = s.mer_d[i];
-        dup = i > 0 && ((id ^ s.mer_id[i - 1]) & kMask) == 0;
+      uint32_t id = 0;
+      int lb = 0;
+      if (t < deg) {
+        d = s.new_d[t];
+        id = s.new_id[t];
+        keep = !full || key_less(d, id, tail_d, tail_id);
+        if (keep) {
+          lb = lower_bound_key(list_d, list_id, 0, sz, d, id);
+          if (lb < sz && ((list_id[lb] ^ id) & kMask) == 0) keep = false;
+        }
       }
-      const unsigned dm = __ballot_sync(kFull, dup);
-      const int pos = i - count - __popc(dm & ((1u << lane) - 1));
-      const bool keep = valid && !dup;
-      if (keep && pos < L) {
-        s.list_id[pos] = id;
-        s.list_d[pos] = d;
+      const unsigned km = __ballot_sync(kFull, keep);
+      if (keep) {
+        const int slot = nsv + __popc(km & ((1u << lane) - 1));
+        s.sv_id[slot] = id;  // unsorted survivors (rank-sorted below)
+        s.sv_d[slot] = d;
+        s.sv_lb[slot] = lb;
       }
-      const unsigned um = __ballot_sync(kFull, keep && !(id & kExpanded));
-      if (best == INT_MAX && um) {
-        const int fl = __ffs(um) - 1;
-        best = base + fl - count - __popc(dm & ((1u << fl) - 1));
-      }
-      count += __popc(dm);
+      nsv += __popc(km);
     }
     __syncwarp();
-    const int C = cap2 - count;
+    // Rank-sort the survivors by key into new_* (ids are distinct, so the
+    // rank is the count of smaller keys); carry the insertion points along.
+    for (int j = lane; j < nsv; j += 32) {
+      const float d = s.sv_d[j];
+      const uint32_t id = s.sv_id[j];
+      int r = 0;
+      for (int f = 0; f < nsv; f++) {
+        const float fd = s.sv_d[f];
+        const uint32_t fi = s.sv_id[f];
+        r += key_less(fd, fi, d, id) || (fd == d && ((fi ^ id) & kMask) == 0 && f < j);
+      }
+      s.new_id[r] = id;
+      s.new_d[r] = d;
+      s.sv_slb[r] = s.sv_lb[j];
+    }
+    __syncwarp();
+    // Old entry i moves to i + #{survivors with insertion point <= i};
+    // survivor r (sorted) goes to its insertion point + r. Positions >= L drop.
+    const int nsz = min(sz + nsv, L);
+    const int32_t* slb = s.sv_slb;
+    if (nsv == 0) {  // list unchanged: keep it in place
+      uint32_t* ti = list_id;
+      float* td = list_d;
+      list_id = out_id_l;
+      list_d = out_d_l;
+      out_id_l = ti;
+      out_d_l = td;
+    }
+    for (int i = lane; nsv && i < sz; i += 32) {
+      int lo = 0, hi = nsv;  // upper_bound of i in the non-decreasing slb
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (slb[mid] <= i) lo = mid + 1; else hi = mid;
+      }
+      const int dst = i + lo;
+      if (dst < L) {
+        out_id_l[dst] = list_id[i];
+        out_d_l[dst] = list_d[i];
+      }
+    }
+    for (int r = lane; r < nsv; r += 32) {
+      const int dst = slb[r] + r;
+      if (dst < L) {
+        out_id_l[dst] = s.new_id[r];
+        out_d_l[dst] = s.new_d[r];
+      }
+    }
+    __syncwarp();
+    // First entry without the expanded bit (pure_mem.cuh:380-419).
+    int best = INT_MAX;
+    for (int base = 0; base < nsz; base += 32) {
+      const int i = base + lane;
+      const unsigned um = __ballot_sync(kFull, i < nsz && !(out_id_l[i] & kExpanded));
+      if (um) {
+        best = base + __ffs(um) - 1;
+        break;
+      }
+    }
     // Exact distance of this node and top-k insertion (pure_mem.cuh:420-424).
     const float ed = warp_exact<T>(s.q, reinterpret_cast<const T*>(node), dim, lane, p.fma_exact);
     topk_push(s.topk_d, s.topk_id, found, k, ed, (int)u, lane);
     hops++;
-    // best == INT_MAX with C < L is where the reference reads stale slots; the
-    // walk stops there. With C >= L the reference stops too.
+    // No unexpanded entry: with a list of L entries the reference stops; with a
+    // shorter list it reads stale slots, and the walk stops here.
     if (best >= L) {
       u = -1;
     } else {
-      u = (int64_t)s.list_id[best];
+      u = (int64_t)out_id_l[best];
       __syncwarp();
-      if (lane == 0) s.list_id[best] |= kExpanded;
-      sz = C < L ? C : L;
+      if (lane == 0) out_id_l[best] |= kExpanded;
+      sz = nsz;
+      // swap the ping-pong lists
+      uint32_t* ti = list_id;
+      float* td = list_d;
+      list_id = out_id_l;
+      list_d = out_d_l;
+      out_id_l = ti;
+      out_d_l = td;
       __syncwarp();
     }
   }
@@ -454,17 +510,7 @@ __global__ void __launch_bounds__(256) plain_search_kernel(PlainParams p, int pe
 }  // namespace
 
 size_t plain_smem_per_warp(int M, int L, int max_m, int k, int dim) {
-  size_t o = 0;
-  o = align16(o + sizeof(float) * (size_t)M * kPivots);
-  o = align16(o + sizeof(float) * dim);
-  o = align16(o + 4 * (size_t)L) ;
-  o = align16(o + 4 * (size_t)L);
-  for (int r = 0; r < 4; r++) o = align16(o + 4 * (size_t)max_m);
-  o = align16(o + 4 * (size_t)(L + max_m));
-  o = align16(o + 4 * (size_t)(L + max_m));
-  o = align16(o + 4 * (size_t)k);
-  o = align16(o + 4 * (size_t)k);
-  return o;
+  return SmemPlan(M, L, max_m, k, dim).total;
 }
 
 cudaError_t launch_plain(const PlainParams& p, int dtype, int num_sms, cudaStream_t stream) {

@@ -211,16 +211,148 @@ def add_reverse_edges(x: torch.Tensor, g: torch.Tensor, R: int, alpha: float, in
     return out
 
 
+def beam_search(x: torch.Tensor, g: torch.Tensor, start: int, qidx: torch.Tensor, L: int,
+                max_iters: int | None = None) -> torch.Tensor:
+    """Batched greedy beam search (Vamana's GreedySearch) from ``start`` for the
+    base points ``qidx``, exact distances, list size L. Returns the expanded
+    nodes of every query, in expansion order (B x iters, -1 padded)."""
+    dev = x.device
+    B = qidx.numel()
+    R = g.shape[1]
+    q = _f32(x[qidx])
+    ids = torch.full((B, L), -1, dtype=torch.long, device=dev)
+    ds = torch.full((B, L), float("inf"), device=dev)
+    ex = torch.zeros((B, L), dtype=torch.bool, device=dev)
+    ids[:, 0] = start
+    ds[:, 0] = ((q - _f32(x[start])[None, :]) ** 2).sum(1)
+    rows = torch.arange(B, device=dev)
+    visited = []
+    max_iters = max_iters or 2 * L
+    for _ in range(max_iters):
+        cand = (~ex) & (ids >= 0)
+        has = cand.any(1)
+        if not bool(has.any()):
+            break
+        pos = torch.argmax(cand.to(torch.int8), 1)
+        u = torch.where(has, ids[rows, pos], torch.full_like(pos, -1))
+        ex[rows[has], pos[has]] = True
+        visited.append(u)
+        nb = g[u.clamp_min(0)]
+        nb = torch.where(has[:, None], nb, torch.full_like(nb, -1))
+        nd = ((_f32(x[nb.clamp_min(0)]) - q[:, None, :]) ** 2).sum(-1)
+        nd[nb < 0] = float("inf")
+        a_id = torch.cat([ids, nb], 1)
+        a_d = torch.cat([ds, nd], 1)
+        a_ex = torch.cat([ex, torch.zeros((B, R), dtype=torch.bool, device=dev)], 1)
+        # drop ids already present (keep the copy that is expanded, else the first)
+        o = torch.argsort(a_id * 2 + (~a_ex).long(), dim=1)
+        s_id = torch.gather(a_id, 1, o)
+        dup = torch.zeros_like(s_id, dtype=torch.bool)
+        dup[:, 1:] = (s_id[:, 1:] == s_id[:, :-1]) & (s_id[:, 1:] >= 0)
+        a_d = a_d.scatter(1, o, torch.where(dup, torch.full_like(a_d, float("inf")), torch.gather(a_d, 1, o)))
+        a_d[a_id < 0] = float("inf")
+        v, sel = torch.topk(a_d, L, dim=1, largest=False)
+        ids = torch.gather(a_id, 1, sel)
+        ex = torch.gather(a_ex, 1, sel)
+        ids[torch.isinf(v)] = -1
+        ds = v
+    return torch.stack(visited, 1) if visited else torch.full((B, 1), -1, dtype=torch.long, device=dev)
+
+
+def vamana_pass(x: torch.Tensor, g: torch.Tensor, start: int, R: int, L: int, alpha: float, rounds: int,
+                seed: int, batch_cap: int = 65536) -> torch.Tensor:
+    """One Vamana pass in ``rounds`` batches: each point searches the current
+    graph from ``start``; its expanded nodes plus its neighbours are pruned
+    with alpha; then reverse edges are offered. The graph is updated after every
+    batch (Vamana updates after every point)."""
+    n = x.shape[0]
+    dev = x.device
+    gen = torch.Generator(device="cpu")
+    gen.manual_seed(seed)
+    order = torch.randperm(n, generator=gen).to(dev)
+    step = min(batch_cap, max(1, (n + rounds - 1) // rounds))
+    for s in range(0, n, step):
+        p = order[s:s + step]
+        vis = beam_search(x, g, start, p, L)
+        cand = torch.cat([vis, g[p]], 1)
+        cand = torch.where(cand == p[:, None], torch.full_like(cand, -1), cand)
+        V = _f32(x[cand.clamp_min(0)])
+        d = ((V - _f32(x[p])[:, None, :]) ** 2).sum(-1)
+        cand, d = _dedupe_sorted(cand, d)
+        g[p] = robust_prune(x, cand, d, R, alpha)
+        g = _offer_reverse(x, g, p, R, alpha)
+    return g
+
+
+def _offer_reverse(x: torch.Tensor, g: torch.Tensor, p: torch.Tensor, R: int, alpha: float) -> torch.Tensor:
+    """For the out-edges p->q of the points p, add q->p; rows over R are pruned."""
+    dev = x.device
+    src = p[:, None].expand(-1, g.shape[1])
+    nb = g[p]
+    m = nb >= 0
+    tgt, back = nb[m], src[m]
+    if tgt.numel() == 0:
+        return g
+    o = torch.argsort(tgt, stable=True)
+    tgt, back = tgt[o], back[o]
+    uniq, cnt = torch.unique_consecutive(tgt, return_counts=True)
+    start = torch.cumsum(cnt, 0) - cnt
+    rank = torch.arange(tgt.numel(), device=dev) - torch.repeat_interleave(start, cnt)
+    cap = int(cnt.max())
+    inc = torch.full((uniq.numel(), cap), -1, dtype=torch.long, device=dev)
+    inc[torch.repeat_interleave(torch.arange(uniq.numel(), device=dev), cnt), rank] = back
+    for s in range(0, uniq.numel(), 16384):
+        u = uniq[s:s + 16384]
+        cand = torch.cat([g[u], inc[s:s + 16384]], 1)
+        V = _f32(x[cand.clamp_min(0)])
+        d = ((V - _f32(x[u])[:, None, :]) ** 2).sum(-1)
+        cand, d = _dedupe_sorted(cand, d)
+        nuniq = (cand >= 0).sum(1)
+        rows = torch.full((u.numel(), R), -1, dtype=torch.long, device=dev)
+        small = nuniq <= R
+        rows[small] = cand[small, :R]
+        if bool((~small).any()):
+            big = torch.nonzero(~small).squeeze(1)
+            rows[big] = robust_prune(x, cand[big], d[big], R, alpha)
+        g[u] = rows
+    return g
+
+
 def build(x: torch.Tensor, R: int, alpha: float = 1.2, K: int | None = None, n_coarse: int | None = None,
-          nprobe: int = 4, seed: int = 7) -> tuple[np.ndarray, np.ndarray, int]:
+          nprobe: int = 4, seed: int = 7, L_build: int = 100, passes: int = 2, rounds: int = 8,
+          random_edges: int = 8) -> tuple[np.ndarray, np.ndarray, int]:
     """Build a graph over the rows of ``x`` (uint8 or float32 tensor).
-    Returns (adjacency n x R int32 padded with -1, degrees n int32, medoid)."""
+    Returns (adjacency n x R int32 padded with -1, degrees n int32, medoid).
+
+    Initial graph: pruned k-NN candidates plus ``random_edges`` random
+    neighbours per node (Vamana starts from a random graph); then ``passes``
+    Vamana passes (alpha 1, then ``alpha``) searching from the medoid with list
+    size ``L_build``."""
     K = K or 2 * R
+    n = x.shape[0]
+    med = medoid(x)
     cand, cand_d = knn_candidates(x, K, n_coarse=n_coarse, nprobe=nprobe, seed=seed)
-    g = robust_prune(x, cand, cand_d, R, alpha)
-    g = add_reverse_edges(x, g, R, alpha)
+    r_loc = max(1, R - random_edges) if n > R + 1 else R
+    g = robust_prune(x, cand, cand_d, r_loc, alpha)
+    if r_loc < R:
+        gen = torch.Generator(device="cpu")
+        gen.manual_seed(seed + 101)
+        rnd = torch.randint(0, n, (n, R - r_loc), generator=gen).to(x.device)
+        self_ = rnd == torch.arange(n, device=x.device)[:, None]
+        rnd = torch.where(self_, (rnd + 1) % n, rnd)
+        g = torch.cat([g, rnd], 1)
+        # remove duplicate targets within each row
+        gd = torch.zeros_like(g, dtype=torch.float32)
+        gs, _ = _dedupe_sorted(g, gd)
+        g = gs[:, :R]
+    for i in range(passes):
+        a = 1.0 if (passes > 1 and i == 0) else alpha
+        g = vamana_pass(x, g, med, R, L_build, a, rounds, seed + 17 * (i + 1))
     deg = (g >= 0).sum(1)
-    return (g.to(torch.int32).cpu().numpy(), deg.to(torch.int32).cpu().numpy(), medoid(x))
+    # neighbours first, -1 padding last
+    o = torch.argsort((g < 0).to(torch.int8), dim=1, stable=True)
+    g = torch.gather(g, 1, o)
+    return (g.to(torch.int32).cpu().numpy(), deg.to(torch.int32).cpu().numpy(), med)
 
 
 def reachable_from(graph: np.ndarray, degrees: np.ndarray, start: int) -> np.ndarray:
