@@ -8,15 +8,20 @@ formats. Search parity is defined on a given index file, so the builder only has
 to produce valid, navigable graphs; it is not meant to match DiskANN edge for
 edge.
 
-Algorithm (GPU-friendly restatement of Vamana's pruning):
-1. candidates: exact k-nearest neighbours for small n; for large n, points are
-   grouped by a coarse k-means and each group searches the members of its
-   ``nprobe`` nearest groups;
-2. RobustPrune with ``alpha`` on squared L2 (a candidate c is dropped when an
-   already kept neighbour j has alpha * d(j, c) < d(p, c));
-3. reverse edges: each kept edge p->q offers q->p; rows that overflow R are
-   pruned again with the same rule.
-The medoid is the point nearest to the mean (DiskANN's entry point).
+Algorithm (a batched, GPU-friendly restatement of Vamana):
+1. initial graph: k-nearest-neighbour candidates (exact for small n; for large n
+   points are grouped by a coarse k-means and each group searches the members of
+   its ``nprobe`` nearest groups) pruned with RobustPrune, plus a few random
+   neighbours per node (Vamana starts from a random graph);
+2. Vamana passes (alpha 1, then ``alpha``): in batches of points, each point
+   runs a greedy beam search (list size ``L_build``) from the medoid on the
+   current graph; its expanded nodes plus its neighbours are pruned with
+   RobustPrune (a candidate c is dropped when an already kept neighbour j has
+   alpha * d(j, c) < d(p, c), squared L2) and every kept edge p->q offers q->p,
+   rows over R being pruned again. The graph is updated after every batch.
+The medoid is the point nearest to the mean (DiskANN's entry point). The
+searches create the long edges that make the graph navigable across the
+well-separated clusters of the synthetic mixtures.
 """
 from __future__ import annotations
 
@@ -129,6 +134,7 @@ def robust_prune(x: torch.Tensor, cand: torch.Tensor, cand_d: torch.Tensor, R: i
     """RobustPrune over rows of candidates sorted by distance (-1 = none).
     Returns n x R int64 neighbour ids (-1 padded), kept in candidate order."""
     n, K = cand.shape
+    batch = max(64, min(batch, int(1.5e9 // (K * K * 4 + K * x.shape[1] * 4))))
     out = torch.full((n, R), -1, dtype=torch.long, device=x.device)
     for s in range(0, n, batch):
         e = min(n, s + batch)
@@ -173,42 +179,6 @@ def _dedupe_sorted(ids: torch.Tensor, d: torch.Tensor):
     d[dup | (ids < 0)] = float("inf")
     o = torch.argsort(d, dim=1, stable=True)
     return torch.gather(ids, 1, o), torch.gather(d, 1, o)
-
-
-def add_reverse_edges(x: torch.Tensor, g: torch.Tensor, R: int, alpha: float, in_cap: int | None = None,
-                      batch: int = 8192) -> torch.Tensor:
-    """Offer every edge p->q back as q->p; rows that overflow R are pruned again."""
-    n = g.shape[0]
-    dev = x.device
-    in_cap = in_cap or R
-    src = torch.arange(n, device=dev)[:, None].expand(-1, g.shape[1])
-    m = g >= 0
-    rs, rd = g[m], src[m]  # reverse edge rs -> rd
-    o = torch.argsort(rs, stable=True)
-    rs, rd = rs[o], rd[o]
-    cnt = torch.bincount(rs, minlength=n)
-    start = torch.cumsum(cnt, 0) - cnt
-    rank = torch.arange(rs.numel(), device=dev) - start[rs]
-    keep = rank < in_cap
-    inc = torch.full((n, in_cap), -1, dtype=torch.long, device=dev)
-    inc[rs[keep], rank[keep]] = rd[keep]
-    out = torch.full((n, R), -1, dtype=torch.long, device=dev)
-    for s in range(0, n, batch):
-        e = min(n, s + batch)
-        cand = torch.cat([g[s:e], inc[s:e]], 1)
-        V = _f32(x[cand.clamp_min(0)])
-        p = _f32(x[s:e])[:, None, :]
-        d = ((V - p) ** 2).sum(-1)
-        cand, d = _dedupe_sorted(cand, d)
-        nuniq = (cand >= 0).sum(1)
-        small = nuniq <= R
-        rows = out[s:e]
-        rows[small] = cand[small, :R]
-        if bool((~small).any()):
-            big = torch.nonzero(~small).squeeze(1)
-            rows[big] = robust_prune(x, cand[big], d[big], R, alpha, batch=batch)
-        out[s:e] = rows
-    return out
 
 
 def beam_search(x: torch.Tensor, g: torch.Tensor, start: int, qidx: torch.Tensor, L: int,
@@ -284,23 +254,34 @@ def vamana_pass(x: torch.Tensor, g: torch.Tensor, start: int, R: int, L: int, al
     return g
 
 
-def _offer_reverse(x: torch.Tensor, g: torch.Tensor, p: torch.Tensor, R: int, alpha: float) -> torch.Tensor:
-    """For the out-edges p->q of the points p, add q->p; rows over R are pruned."""
+def _offer_reverse(x: torch.Tensor, g: torch.Tensor, p: torch.Tensor, R: int, alpha: float,
+                   in_cap: int | None = None) -> torch.Tensor:
+    """For the out-edges p->q of the points p, add q->p; rows over R are pruned.
+    Each q considers at most ``in_cap`` (default 2R) of its new in-edges, the
+    nearest ones."""
     dev = x.device
+    in_cap = in_cap or 2 * R
     src = p[:, None].expand(-1, g.shape[1])
     nb = g[p]
     m = nb >= 0
     tgt, back = nb[m], src[m]
     if tgt.numel() == 0:
         return g
-    o = torch.argsort(tgt, stable=True)
+    ed = torch.empty(tgt.numel(), dtype=torch.float32, device=dev)
+    for s in range(0, tgt.numel(), 1 << 20):
+        ed[s:s + (1 << 20)] = ((_f32(x[tgt[s:s + (1 << 20)]]) - _f32(x[back[s:s + (1 << 20)]])) ** 2).sum(1)
+    o = torch.argsort(ed, stable=True)
+    tgt, back = tgt[o], back[o]
+    o = torch.argsort(tgt, stable=True)  # by target, nearest first within a target
     tgt, back = tgt[o], back[o]
     uniq, cnt = torch.unique_consecutive(tgt, return_counts=True)
     start = torch.cumsum(cnt, 0) - cnt
     rank = torch.arange(tgt.numel(), device=dev) - torch.repeat_interleave(start, cnt)
-    cap = int(cnt.max())
+    keep = rank < in_cap
+    cap = int(min(int(cnt.max()), in_cap))
     inc = torch.full((uniq.numel(), cap), -1, dtype=torch.long, device=dev)
-    inc[torch.repeat_interleave(torch.arange(uniq.numel(), device=dev), cnt), rank] = back
+    rowi = torch.repeat_interleave(torch.arange(uniq.numel(), device=dev), cnt)
+    inc[rowi[keep], rank[keep]] = back[keep]
     for s in range(0, uniq.numel(), 16384):
         u = uniq[s:s + 16384]
         cand = torch.cat([g[u], inc[s:s + 16384]], 1)
