@@ -185,7 +185,10 @@ def recall_at(ids: np.ndarray, gt: np.ndarray, k: int) -> float:
 
 
 class PlainRunner:
-    """gann_search_device_ex on resident device buffers (the `value` path)."""
+    """gann_search_device_ex on resident device buffers (the reference-semantics form)."""
+
+    name = "plain"
+    launches_per_step = 1
 
     def __init__(self, g, q_dev, k):
         import torch
@@ -207,7 +210,45 @@ class PlainRunner:
                                 self.fnd.data_ptr(), self.hops.data_ptr() if counters else 0,
                                 self.bytes.data_ptr() if counters else 0, s)
 
-    launches_per_step = 1
+    def host_call(self, q_pinned, L, outs, t):
+        import ctypes
+
+        import gustann_b200 as gb
+
+        ids, dis, fnd = outs
+        gb._check(gb.lib().gann_search(self.g.handle, q_pinned.data_ptr(), self.nq, self.k, L, ids.data_ptr(),
+                                       dis.data_ptr(), fnd.data_ptr(), ctypes.byref(t)))
+
+
+class BatchRunner(PlainRunner):
+    """gann_search_batch_device: W nodes per step, visited cache, BF16/FP32 tables."""
+
+    def __init__(self, g, q_dev, k, precision, beam_width, name):
+        super().__init__(g, q_dev, k)
+        self.precision, self.W, self.name = precision, beam_width, name
+        import gustann_b200 as gb
+
+        self.launches_per_step = 2 if precision in (gb.PREC_BF16, gb.PREC_BF16X3) else 1
+
+    def run(self, L, counters=False):
+        import torch
+
+        s = torch.cuda.current_stream().cuda_stream
+        self.g.search_batch_device(self.q.data_ptr(), self.nq, 0, 0, self.k, L, self.ids.data_ptr(),
+                                   self.dis.data_ptr(), self.fnd.data_ptr(),
+                                   self.hops.data_ptr() if counters else 0, self.bytes.data_ptr() if counters else 0,
+                                   precision=self.precision, beam_width=self.W, stream=s)
+
+    def host_call(self, q_pinned, L, outs, t):
+        import ctypes
+
+        import gustann_b200 as gb
+
+        ids, dis, fnd = outs
+        o = gb.GustANN._opts(self.precision, self.W, 0)
+        gb._check(gb.lib().gann_search_batch(self.g.handle, q_pinned.data_ptr(), self.nq, None, None, self.k, L,
+                                             ctypes.byref(o), ids.data_ptr(), dis.data_ptr(), fnd.data_ptr(),
+                                             ctypes.byref(t)))
 
 
 def calibrate(runner, gt, k, target, fixed_L=None):
@@ -251,32 +292,24 @@ def time_steps(runner, L, steps, warmup, world, flush):
     return times
 
 
-def e2e_steps(g, q_host_pinned, k, L, steps, warmup):
-    """Public host-buffer API (gann_search): H2D of the queries and D2H of the
-    results inside every step."""
-    nq = q_host_pinned.shape[0]
-    import torch
-
-    ids = torch.zeros((nq, k), dtype=torch.int32).pin_memory()
-    dis = torch.zeros((nq, k), dtype=torch.float32).pin_memory()
-    fnd = torch.zeros(nq, dtype=torch.int32).pin_memory()
+def e2e_steps(runner, q_host_pinned, L, steps, warmup):
+    """The public host-buffer API: H2D of the queries and D2H of the results
+    inside every step."""
     import ctypes
 
-    import gustann_b200 as gb
+    import torch
 
+    nq, k = runner.nq, runner.k
+    outs = (torch.zeros((nq, k), dtype=torch.int32).pin_memory(),
+            torch.zeros((nq, k), dtype=torch.float32).pin_memory(),
+            torch.zeros(nq, dtype=torch.int32).pin_memory())
     t = ctypes.c_double()
-
-    def one():
-        rc = gb.lib().gann_search(g.handle, q_host_pinned.data_ptr(), nq, k, L, ids.data_ptr(), dis.data_ptr(),
-                                  fnd.data_ptr(), ctypes.byref(t))
-        gb._check(rc)
-
     for _ in range(warmup):
-        one()
+        runner.host_call(q_host_pinned, L, outs, t)
     ts = []
     for _ in range(steps):
         t0 = time.perf_counter()
-        one()
+        runner.host_call(q_host_pinned, L, outs, t)
         ts.append(time.perf_counter() - t0)
     h2d = nq * q_host_pinned.shape[1] * 4
     d2h = nq * k * 8 + nq * 4
@@ -333,6 +366,24 @@ def run_ours(args, rank, world, local):
         _run_ours(args, rank, world, local)
 
 
+def measure_form(runner, args, gt, world, flush, local):
+    import torch
+
+    L, rec = calibrate(runner, gt, args.k, args.recall, args.L or None)
+    runner.run(L, counters=True)
+    torch.cuda.synchronize()
+    hops = runner.hops.cpu().numpy()
+    step_bytes = int(runner.bytes.sum().item())
+    clocks = ClockSampler(local)
+    clocks.start()
+    times_ms = time_steps(runner, L, args.steps, args.warmup, world, flush)
+    clk = clocks.stop()
+    total_ms = max_over_ranks(float(sum(times_ms)), world, device="cuda")
+    return {"L": L, "recall": rec, "total_ms": total_ms, "avg_ms": float(np.mean(times_ms)),
+            "qps": world * runner.nq * args.steps / (total_ms / 1e3), "hops_per_query": float(hops.mean()),
+            "bytes_per_step": step_bytes, "clocks": clk}
+
+
 def _run_ours(args, rank, world, local):
     import torch
 
@@ -347,54 +398,54 @@ def _run_ours(args, rank, world, local):
     q = torch.from_numpy(meta["queries"]).cuda()
     gt = meta["gt"]
     k = args.k
-    runner = PlainRunner(g, q, k)
-    L, rec = calibrate(runner, gt, k, args.recall, args.L)
-    # device counters: hops and algorithmic bytes of one step (same work every step)
-    runner.run(L, counters=True)
-    torch.cuda.synchronize()
-    hops = runner.hops.cpu().numpy()
-    step_bytes = int(runner.bytes.sum().item())
+    runners = {"plain": PlainRunner(g, q, k),
+               "batched_bf16": BatchRunner(g, q, k, gb.PREC_BF16, args.beam, "batched_bf16"),
+               "batched_bf16x3": BatchRunner(g, q, k, gb.PREC_BF16X3, args.beam, "batched_bf16x3"),
+               "batched_fp32": BatchRunner(g, q, k, gb.PREC_FP32, args.beam, "batched_fp32")}
+    forms = [f for f in args.forms.split(",") if f in runners]
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-    clocks = ClockSampler(local)
-    clocks.start()
-    times_ms = time_steps(runner, L, args.steps, args.warmup, world, flush)
-    clk = clocks.stop()
-    total_ms = max_over_ranks(float(sum(times_ms)), world, device="cuda")
+    res = {f: measure_form(runners[f], args, gt, world, flush, local) for f in forms}
+    ok = [f for f in forms if res[f]["recall"] >= args.recall]
+    head = args.headline if args.headline in ok else (max(ok, key=lambda f: res[f]["qps"]) if ok else forms[0])
+    r, runner = res[head], runners[head]
     nq = runner.nq
-    value = world * nq * args.steps / (total_ms / 1e3)
-    avg_ms = float(np.mean(times_ms))
     peak, peak_kind = load_peaks()
-    achieved = step_bytes / (avg_ms / 1e3) / 1e9
-    tpq = traffic_per_query("plain_search_kernel", args.workload)
-    # end to end through the public host API
+    achieved = r["bytes_per_step"] / (r["avg_ms"] / 1e3) / 1e9
+    tpq = traffic_per_query("batch_search_kernel" if head != "plain" else "plain_search_kernel", args.workload)
     qp = torch.from_numpy(meta["queries"]).pin_memory()
-    e2e_val, h2d, d2h = e2e_steps(g, qp, k, L, max(2, min(args.steps, 5)), 1)
+    e2e_val, h2d, d2h = e2e_steps(runner, qp, r["L"], max(2, min(args.steps, 5)), 1)
     e2e_total = max_over_ranks(1.0 / e2e_val, world, device="cuda")
     out = {
-        "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "metric": METRIC, "value": r["qps"], "unit": "queries/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": r["total_ms"] / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "bf16" if "bf16" in head else "f32",
         "data": f"synthetic seeded Gaussian mixture ({meta['clusters']} clusters) standing in for "
                 f"{'SIFT' if meta['kind'] == 'u8' else 'DEEP'}; index built on the device",
         "config": {"workload": args.workload, "n": meta["n"], "dim": meta["dim"], "vector": meta["kind"],
                    "R": meta["R"], "pq_chunks": meta["M"], "nav_points": meta["nav"], "queries_per_step": nq,
-                   "k": k, "L": L, "form": "plain", "l2": "flushed (256 MB write) before every step",
-                   "parallelism": f"replicas x{world}"},
-        "recall": rec, "recall_target": args.recall,
-        "hops_per_query": float(hops.mean()),
-        "gathered_bytes_per_query": step_bytes / nq,
+                   "k": k, "L": r["L"], "form": head, "beam_width": args.beam if head != "plain" else 1,
+                   "l2": "flushed (256 MB write) before every step", "parallelism": f"replicas x{world}"},
+        "recall": r["recall"], "recall_target": args.recall,
+        "hops_per_query": r["hops_per_query"],
+        "gathered_bytes_per_query": r["bytes_per_step"] / nq,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak if peak else None,
                      "traffic": None if tpq is None else tpq * nq, "peak_kind": peak_kind,
-                     "kernel": "plain_search_kernel"},
+                     "kernel": "batch_search_kernel" if head != "plain" else "plain_search_kernel"},
         "e2e": {"value": world / e2e_total, "unit": "queries/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": runner.launches_per_step * args.steps,
-        "clocks": clk,
+        "clocks": r["clocks"],
+        "forms": {f: {"qps": v["qps"], "L": v["L"], "recall": v["recall"], "ms_per_step": v["total_ms"] / args.steps,
+                      "hops_per_query": v["hops_per_query"], "gathered_bytes_per_query": v["bytes_per_step"] / nq}
+                  for f, v in res.items()},
         "build_s": meta.get("build_s"),
     }
+    if "plain" in res and head != "plain":
+        out["speedup_vs_plain"] = r["qps"] / res["plain"]["qps"]
     if rank == 0 and world == 1 and not args.no_cpu:
-        out["cpu_baseline"], _ = cpu_baseline(meta, L, k, args.cpu_budget)
+        L_ref = res["plain"]["L"] if "plain" in res else r["L"]
+        out["cpu_baseline"], _ = cpu_baseline(meta, L_ref, k, args.cpu_budget)
     g.close()
     barrier(world)
     if world > 1:
@@ -491,7 +542,7 @@ def run_reference(args, rank, world, local):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=list(WORKLOADS), default="c0")
@@ -503,6 +554,9 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true")
+    ap.add_argument("--forms", default="plain,batched_bf16,batched_bf16x3,batched_fp32")
+    ap.add_argument("--headline", default="batched_bf16")
+    ap.add_argument("--beam", type=int, default=4)
     args = ap.parse_args()
     rank, world, local = dist_env()
     if args.impl == "reference":

@@ -25,7 +25,7 @@ _LIB_PATH = Path(__file__).resolve().parent / "libgann.so"
 _lib = None
 
 GANN_OK, GANN_EINVAL, GANN_EIO, GANN_EFORMAT, GANN_ECUDA, GANN_ENOMEM, GANN_EKERNEL, GANN_ERANGE = range(8)
-PREC_FP32, PREC_BF16, PREC_BF16X3 = 0, 1, 2
+PREC_FP32, PREC_BF16, PREC_BF16X3, PREC_BF16_CC = 0, 1, 2, 3
 
 
 class DataType(enum.IntEnum):
@@ -57,6 +57,13 @@ class GustANNError(RuntimeError):
         self.code = code
 
 
+class BatchOpts(ctypes.Structure):
+    """gann_batch_opts_t (include/gann.h)."""
+
+    _fields_ = [("precision", ctypes.c_int32), ("beam_width", ctypes.c_int32), ("hash_bits", ctypes.c_int32),
+                ("reserved", ctypes.c_int32 * 5)]
+
+
 class GannInfo(ctypes.Structure):
     _fields_ = [
         ("num_points", ctypes.c_int64), ("dim", ctypes.c_int64), ("max_degree", ctypes.c_int64),
@@ -76,6 +83,9 @@ _SIGNATURES = {
     "gann_search": (_I, [_P, _P, _I, _I, _I, _P, _P, _P, ctypes.POINTER(ctypes.c_double)]),
     "gann_search_device": (_I, [_P, _P, _I, _I, _I, _P, _P, _P, _P]),
     "gann_search_device_ex": (_I, [_P, _P, _I, _I, _I, _P, _P, _P, _P, _P, _P]),
+    "gann_search_batch": (_I, [_P, _P, _I, _P, _P, _I, _I, _P, _P, _P, _P, ctypes.POINTER(ctypes.c_double)]),
+    "gann_search_batch_device": (_I, [_P, _P, _I, _P, _P, _I, _I, _P, _P, _P, _P, _P, _P, _P]),
+    "gann_pq_tables": (_I, [_P, _P, _I, _I, _P]),
     "gann_check": (_I, [_P, _P]),
     "gann_set_fma": (_I, [_P, _I, _I]),
     "gann_last_error": (ctypes.c_char_p, []),
@@ -206,6 +216,49 @@ class GustANN:
         """gann_search_device_ex: also writes per-query hop and gathered-byte counters."""
         _check(lib().gann_search_device_ex(self.handle, d_q, nq, topk, ef_search, d_nns, d_dists, d_found,
                                            d_hops or None, d_bytes or None, _stream(stream)))
+
+    @staticmethod
+    def _opts(precision, beam_width, hash_bits):
+        o = BatchOpts()
+        o.precision, o.beam_width, o.hash_bits = int(precision), int(beam_width), int(hash_bits)
+        return o
+
+    def search_batch(self, q: np.ndarray, topk, ef_search, precision: int = PREC_BF16, beam_width: int = 0,
+                     hash_bits: int = 0):
+        """Batched search (gann_search_batch). ``topk`` / ``ef_search`` are ints or
+        per-query int arrays. Returns (ids nq x kmax, distances, found, seconds)."""
+        q = np.ascontiguousarray(q, dtype=np.float32)
+        nq = q.shape[0]
+        karr = None if np.isscalar(topk) else np.ascontiguousarray(topk, dtype=np.int32)
+        larr = None if np.isscalar(ef_search) else np.ascontiguousarray(ef_search, dtype=np.int32)
+        kmax = int(topk) if karr is None else int(karr.max(initial=1))
+        lmax = int(ef_search) if larr is None else int(larr.max(initial=1))
+        nns = np.zeros((nq, kmax), np.int32)
+        dis = np.zeros((nq, kmax), np.float32)
+        fnd = np.zeros(nq, np.int32)
+        t = ctypes.c_double(0.0)
+        o = self._opts(precision, beam_width, hash_bits)
+        _check(lib().gann_search_batch(self.handle, _ptr(q), nq, None if karr is None else _ptr(karr),
+                                       None if larr is None else _ptr(larr), kmax, lmax, ctypes.byref(o),
+                                       _ptr(nns), _ptr(dis), _ptr(fnd), ctypes.byref(t)))
+        return nns, dis, fnd, t.value
+
+    def search_batch_device(self, d_q: int, nq: int, d_topk: int, d_ef: int, topk_max: int, ef_max: int,
+                            d_nns: int, d_dists: int, d_found: int, d_hops: int = 0, d_bytes: int = 0,
+                            precision: int = PREC_BF16, beam_width: int = 0, hash_bits: int = 0,
+                            stream: int | None = None) -> None:
+        o = self._opts(precision, beam_width, hash_bits)
+        _check(lib().gann_search_batch_device(self.handle, d_q, nq, d_topk or None, d_ef or None, topk_max, ef_max,
+                                              ctypes.byref(o), d_nns, d_dists, d_found, d_hops or None,
+                                              d_bytes or None, _stream(stream)))
+
+    def pq_tables(self, q: np.ndarray, precision: int) -> np.ndarray:
+        """PQ tables (nq x M x 256, FP32 view) as the given precision builds them."""
+        q = np.ascontiguousarray(q, dtype=np.float32)
+        M = self.info()["pq_chunks"]
+        out = np.zeros((q.shape[0], M, 256), np.float32)
+        _check(lib().gann_pq_tables(self.handle, _ptr(q), q.shape[0], int(precision), _ptr(out)))
+        return out
 
     def check(self, stream: int | None = None) -> None:
         _check(lib().gann_check(self.handle, _stream(stream)))

@@ -108,8 +108,11 @@ __global__ void validate_records(const uint8_t* pages, int64_t n, int64_t npp, i
 void free_all(gann_index* h) {
   for (void* p : h->allocations) cudaFree(p);
   h->allocations.clear();
-  for (void* p : {(void*)h->d_q, (void*)h->d_nns, (void*)h->d_dists, (void*)h->d_found})
+  for (void* p : {(void*)h->d_q, (void*)h->d_nns, (void*)h->d_dists, (void*)h->d_found, (void*)h->d_kq,
+                  (void*)h->d_lq, (void*)h->d_tables})
     if (p) cudaFree(p);
+  h->d_kq = h->d_lq = nullptr;
+  h->d_tables = nullptr;
   h->d_q = nullptr;
   h->d_nns = nullptr;
   h->d_dists = nullptr;
@@ -230,8 +233,22 @@ int gann_open(const char* index_file, const char* pq_prefix, const char* nav_dir
       h->dx.nav_graph = upload(h.get(), hx.nav_graph);
       h->dx.nav_map = upload(h.get(), hx.nav_map);
     }
+    {  // operands of the tensor-core table build, when every chunk is at most 16 wide
+      std::vector<uint8_t> bhi, blo;
+      std::vector<float> pn;
+      int tp = 0, tg = 0;
+      if (gann::make_tc_panels(hx.pivots, hx.chunk_offsets, (int)hx.dim, bhi, blo, pn, tp, tg) &&
+          gann::table_tc_smem(hx.pq_m, tg) <= 227 * 1024) {
+        h->dx.tc_bpanel_hi = upload(h.get(), bhi);
+        h->dx.tc_bpanel_lo = upload(h.get(), blo);
+        h->dx.tc_pnorm = upload(h.get(), pn);
+        h->dx.tc_p = tp;
+        h->dx.tc_groups = tg;
+      }
+    }
     h->d_counter = dev_alloc<int>(h.get(), 1);
     h->d_err = dev_alloc<unsigned int>(h.get(), 1);
+    h->dx.err = h->d_err;
     ck(cudaMemset(h->d_err, 0, sizeof(unsigned int)), "cudaMemset");
     if (!(flags & GANN_OPEN_NO_VALIDATE)) {
       unsigned long long* bad = dev_alloc<unsigned long long>(h.get(), 1);
@@ -357,6 +374,217 @@ int gann_search(gann_t* h, const float* queries, int nq, int topk, int ef_search
     if (run_time) *run_time = ms * 1e-3;
   } catch (const CudaFail& e) {
     return set_error(GANN_ECUDA, std::string(e.what) + ": " + cudaGetErrorString(e.e));
+  }
+  return GANN_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+int batch_hash_bits(int ef_max) {
+  int b = 9;
+  while ((1 << b) < 4 * ef_max && b < 13) b++;
+  return b;
+}
+
+int enqueue_batch(gann_t* h, const float* d_q, int nq, const int32_t* d_k, const int32_t* d_l, int k_max,
+                  int l_max, const gann_batch_opts_t* opts, int32_t* d_nns, float* d_dists, int32_t* d_found,
+                  int32_t* d_hops, int64_t* d_bytes, cudaStream_t s) {
+  gann_batch_opts_t o{};
+  if (opts) o = *opts;
+  const int prec = opts ? o.precision : GANN_PREC_BF16;
+  const int W = o.beam_width ? o.beam_width : 4;
+  if (!(W == 1 || W == 2 || W == 4 || W == 8)) return set_error(GANN_EINVAL, "beam_width must be 1, 2, 4 or 8");
+  if (prec < GANN_PREC_FP32 || prec > GANN_PREC_BF16_CC) return set_error(GANN_EINVAL, "unknown precision");
+  const int hb = o.hash_bits ? o.hash_bits : batch_hash_bits(l_max);
+  if (hb < 4 || hb > 16) return set_error(GANN_EINVAL, "hash_bits must be in 4..16");
+  const bool bf16 = prec != GANN_PREC_FP32;
+  const size_t smem = gann::batch_smem_bytes(h->hx.pq_m, bf16 ? 2 : 4, hb, l_max, (int)h->hx.max_m0, W, k_max,
+                                             (int)h->hx.dim);
+  if (smem > 227 * 1024)
+    return set_error(GANN_ERANGE, "table + lists + visited cache of one query exceed 227 KB of shared memory");
+  gann::BatchParams p{};
+  p.ix = h->dx;
+  p.n = h->hx.n;
+  p.npp = h->hx.npp;
+  p.node_len = h->hx.node_len;
+  p.data_len = h->hx.data_len;
+  p.medoid = h->hx.medoid;
+  p.dim = (int)h->hx.dim;
+  p.max_m = (int)h->hx.max_m0;
+  p.M = h->hx.pq_m;
+  p.has_nav = h->hx.has_nav;
+  p.nav_n = h->hx.nav_n;
+  p.nav_max_m = h->hx.nav_max_m;
+  p.nav_start = h->hx.nav_start;
+  p.queries = d_q;
+  p.nq = nq;
+  p.L_per_q = d_l;
+  p.k_per_q = d_k;
+  p.L_max = l_max;
+  p.k_max = k_max;
+  p.hash_bits = hb;
+  p.fma = h->fma_exact;
+  p.nns = d_nns;
+  p.dists = d_dists;
+  p.found = d_found;
+  p.hops = d_hops;
+  p.bytes = d_bytes;
+  p.next_query = h->d_counter;
+  p.err = h->d_err;
+  cudaError_t e = cudaSuccess;
+  if ((prec == GANN_PREC_BF16 || prec == GANN_PREC_BF16X3) && !h->dx.tc_bpanel_hi)
+    return set_error(GANN_ERANGE, "tensor-core tables need PQ chunks of at most 16 dimensions");
+  if (prec == GANN_PREC_BF16 || prec == GANN_PREC_BF16X3) {
+    const size_t need = (size_t)nq * h->hx.pq_m * gann::kPivots;
+    if (need > h->cap_tables) {
+      if (h->d_tables) cudaFree(h->d_tables);
+      h->d_tables = nullptr;
+      h->cap_tables = 0;
+      e = cudaMalloc(&h->d_tables, need * sizeof(__nv_bfloat16));
+      if (e != cudaSuccess) return set_error(GANN_ENOMEM, "cannot allocate the batch's BF16 tables");
+      h->cap_tables = need;
+    }
+    e = gann::launch_table_tc(h->dx, (int)h->hx.dim, h->hx.pq_m, d_q, nq, prec == GANN_PREC_BF16X3, h->d_tables, s);
+    if (e != cudaSuccess) return set_error(GANN_ECUDA, std::string("table build: ") + cudaGetErrorString(e));
+    p.tables = h->d_tables;
+  }
+  if (d_bytes) e = cudaMemsetAsync(d_bytes, 0, sizeof(int64_t) * nq, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->d_counter, 0, sizeof(int), s);
+  if (e == cudaSuccess) e = gann::launch_batch(p, h->hx.dtype, bf16, W, h->num_sms, s);
+  if (e != cudaSuccess) return set_error(GANN_ECUDA, std::string("batch search launch: ") + cudaGetErrorString(e));
+  return GANN_OK;
+}
+
+int check_batch_args(const gann_t* h, int nq, int k_max, int l_max) {
+  if (!h) return set_error(GANN_EINVAL, "null handle");
+  if (nq < 0) return set_error(GANN_EINVAL, "nq must be >= 0");
+  if (k_max < 1 || l_max < 1) return set_error(GANN_EINVAL, "topk_max and ef_max must be >= 1");
+  if (k_max > 4096 || l_max > 4096) return set_error(GANN_ERANGE, "topk and ef_search are limited to 4096");
+  return GANN_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gann_search_batch_device(gann_t* h, const float* d_queries, int nq, const int32_t* d_topk,
+                             const int32_t* d_ef_search, int topk_max, int ef_max, const gann_batch_opts_t* opts,
+                             int32_t* d_nns, float* d_distances, int32_t* d_found_cnt, int32_t* d_hops,
+                             int64_t* d_bytes, void* stream) {
+  int rc = check_batch_args(h, nq, topk_max, ef_max);
+  if (rc) return rc;
+  if (nq == 0) return GANN_OK;
+  if (!d_queries || !d_nns || !d_distances || !d_found_cnt) return set_error(GANN_EINVAL, "null buffer");
+  std::lock_guard<std::mutex> lk(h->mu);
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
+  return enqueue_batch(h, d_queries, nq, d_topk, d_ef_search, topk_max, ef_max, opts, d_nns, d_distances,
+                       d_found_cnt, d_hops, d_bytes, s);
+}
+
+int gann_search_batch(gann_t* h, const float* queries, int nq, const int32_t* topk, const int32_t* ef_search,
+                      int topk_max, int ef_max, const gann_batch_opts_t* opts, int32_t* nns, float* distances,
+                      int32_t* found_cnt, double* run_time) {
+  if (run_time) *run_time = 0.0;
+  if (h && nq > 0 && topk) {
+    int m = 0;
+    for (int i = 0; i < nq; i++) m = topk[i] > m ? topk[i] : m;
+    if (m > topk_max) return set_error(GANN_EINVAL, "a topk entry exceeds topk_max");
+  }
+  if (h && nq > 0 && ef_search) {
+    int m = 0;
+    for (int i = 0; i < nq; i++) m = ef_search[i] > m ? ef_search[i] : m;
+    if (m > ef_max) return set_error(GANN_EINVAL, "an ef_search entry exceeds ef_max");
+  }
+  int rc = check_batch_args(h, nq, topk_max, ef_max);
+  if (rc) return rc;
+  if (nq == 0) return GANN_OK;
+  if (!queries || !nns || !distances || !found_cnt) return set_error(GANN_EINVAL, "null buffer");
+  std::lock_guard<std::mutex> lk(h->mu);
+  try {
+    const size_t qn = (size_t)nq * h->hx.dim, on = (size_t)nq * topk_max;
+    grow(h->d_q, h->cap_q, qn);
+    grow(h->d_nns, h->cap_out, on);
+    grow(h->d_dists, h->cap_dists, on);
+    grow(h->d_found, h->cap_found, (size_t)nq);
+    cudaStream_t s = h->stream;
+    ck(cudaMemcpyAsync(h->d_q, queries, sizeof(float) * qn, cudaMemcpyHostToDevice, s), "query upload");
+    int32_t *dk = nullptr, *dl = nullptr;
+    if (topk) {
+      grow(h->d_kq, h->cap_kq, (size_t)nq);
+      ck(cudaMemcpyAsync(h->d_kq, topk, sizeof(int32_t) * nq, cudaMemcpyHostToDevice, s), "topk upload");
+      dk = h->d_kq;
+    }
+    if (ef_search) {
+      grow(h->d_lq, h->cap_lq, (size_t)nq);
+      ck(cudaMemcpyAsync(h->d_lq, ef_search, sizeof(int32_t) * nq, cudaMemcpyHostToDevice, s), "L upload");
+      dl = h->d_lq;
+    }
+    ck(cudaEventRecord(h->ev0, s), "cudaEventRecord");
+    rc = enqueue_batch(h, h->d_q, nq, dk, dl, topk_max, ef_max, opts, h->d_nns, h->d_dists, h->d_found, nullptr,
+                       nullptr, s);
+    if (rc) return rc;
+    ck(cudaEventRecord(h->ev1, s), "cudaEventRecord");
+    ck(cudaMemcpyAsync(nns, h->d_nns, sizeof(int32_t) * on, cudaMemcpyDeviceToHost, s), "result download");
+    ck(cudaMemcpyAsync(distances, h->d_dists, sizeof(float) * on, cudaMemcpyDeviceToHost, s), "result download");
+    ck(cudaMemcpyAsync(found_cnt, h->d_found, sizeof(int32_t) * nq, cudaMemcpyDeviceToHost, s), "result download");
+    unsigned int err = 0;
+    ck(cudaMemcpyAsync(&err, h->d_err, sizeof(err), cudaMemcpyDeviceToHost, s), "error word");
+    ck(cudaStreamSynchronize(s), "batch search");
+    if (err) {
+      ck(cudaMemset(h->d_err, 0, sizeof(unsigned int)), "cudaMemset");
+      return kernel_error_status(err);
+    }
+    float ms = 0.0f;
+    ck(cudaEventElapsedTime(&ms, h->ev0, h->ev1), "cudaEventElapsedTime");
+    if (run_time) *run_time = ms * 1e-3;
+  } catch (const CudaFail& e) {
+    return set_error(GANN_ECUDA, std::string(e.what) + ": " + cudaGetErrorString(e.e));
+  }
+  return GANN_OK;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+int gann_pq_tables(gann_t* h, const float* queries, int nq, int precision, float* tables) {
+  if (!h || nq < 0 || (nq && (!queries || !tables))) return set_error(GANN_EINVAL, "bad argument");
+  if (precision < GANN_PREC_FP32 || precision > GANN_PREC_BF16_CC) return set_error(GANN_EINVAL, "unknown precision");
+  if (nq == 0) return GANN_OK;
+  if ((precision == GANN_PREC_BF16 || precision == GANN_PREC_BF16X3) && !h->dx.tc_bpanel_hi)
+    return set_error(GANN_ERANGE, "tensor-core tables need PQ chunks of at most 16 dimensions");
+  std::lock_guard<std::mutex> lk(h->mu);
+  const size_t qn = (size_t)nq * h->hx.dim, tn = (size_t)nq * h->hx.pq_m * gann::kPivots;
+  float* dq = nullptr;
+  float* dt = nullptr;
+  __nv_bfloat16* db = nullptr;
+  cudaStream_t s = h->stream;
+  cudaError_t e = cudaMalloc(&dq, qn * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&dt, tn * sizeof(float));
+  if (e == cudaSuccess && precision != GANN_PREC_FP32) e = cudaMalloc(&db, tn * sizeof(__nv_bfloat16));
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dq, queries, qn * sizeof(float), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) {
+    if (precision == GANN_PREC_FP32)
+      e = gann::launch_table_cc(h->dx, (int)h->hx.dim, h->hx.pq_m, dq, nq, h->fma_table, false, dt, s);
+    else if (precision == GANN_PREC_BF16_CC)
+      e = gann::launch_table_cc(h->dx, (int)h->hx.dim, h->hx.pq_m, dq, nq, h->fma_table, true, db, s);
+    else
+      e = gann::launch_table_tc(h->dx, (int)h->hx.dim, h->hx.pq_m, dq, nq, precision == GANN_PREC_BF16X3, db, s);
+  }
+  if (e == cudaSuccess && db) e = gann::widen_bf16(db, dt, tn, s);
+  unsigned int err = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(tables, dt, tn * sizeof(float), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&err, h->d_err, sizeof(err), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaFree(dq);
+  cudaFree(dt);
+  if (db) cudaFree(db);
+  if (e != cudaSuccess) return set_error(GANN_ECUDA, std::string("gann_pq_tables: ") + cudaGetErrorString(e));
+  if (err) {
+    cudaMemset(h->d_err, 0, sizeof(unsigned int));
+    return kernel_error_status(err);
   }
   return GANN_OK;
 }

@@ -1,6 +1,7 @@
 // Internal types shared by the host side and the kernels of libgann.
 #pragma once
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -53,6 +54,12 @@ struct DeviceIndex {
   const uint8_t* nav_data = nullptr;   // nav_n x dim x elt
   const int32_t* nav_graph = nullptr;  // nav_n x nav_max_m
   const int32_t* nav_map = nullptr;    // nav_n
+  // tensor-core table build (table_tc.cu): B operand tiles, centroid norms
+  const uint8_t* tc_bpanel_hi = nullptr;  // M x 8 KB
+  const uint8_t* tc_bpanel_lo = nullptr;  // M x 8 KB
+  const float* tc_pnorm = nullptr;        // M x 256
+  int tc_p = 0, tc_groups = 0;            // padded chunk width, chunk groups per K=16 slice
+  unsigned int* err = nullptr;            // kernel error word
 };
 
 // Launch parameters of the plain search kernel (walk_plain.cu).
@@ -72,6 +79,48 @@ struct PlainParams {
   int* next_query;           // work counter, zeroed before launch
   unsigned int* err;         // error word
 };
+
+// Launch parameters of the batched search kernel (walk_batch.cu).
+struct BatchParams {
+  DeviceIndex ix;
+  int64_t n, npp, node_len, data_len, medoid;
+  int dim, max_m, M;
+  int has_nav, nav_n, nav_max_m, nav_start;
+  const float* queries;           // nq x dim
+  int nq;
+  const int32_t* L_per_q;         // nq or null (then L_max for all)
+  const int32_t* k_per_q;         // nq or null (then k_max for all)
+  int L_max, k_max;
+  int hash_bits;                  // visited cache: 1 << hash_bits slots
+  const __nv_bfloat16* tables;    // nq x M x 256 BF16 tables built for the batch, or null
+  int fma;
+  int32_t* nns;                   // nq x k_max
+  float* dists;                   // nq x k_max
+  int32_t* found;                 // nq
+  int32_t* hops;                  // nq or null
+  int64_t* bytes;                 // nq or null (accumulated; zeroed by the caller)
+  int* next_query;                // work counter, zeroed before launch
+  unsigned int* err;
+};
+
+size_t batch_smem_bytes(int M, int tab_bytes, int hash_bits, int L_max, int max_m, int W, int k_max, int dim);
+cudaError_t launch_batch(const BatchParams& p, int dtype, int table_bf16, int W, int num_sms, cudaStream_t stream);
+
+// CUDA-core tables (FP32 or BF16 storage) of a query batch, one warp per query.
+cudaError_t launch_table_cc(const DeviceIndex& ix, int dim, int M, const float* queries, int nq, int fma,
+                            bool bf16, void* tables, cudaStream_t stream);
+cudaError_t widen_bf16(const __nv_bfloat16* in, float* out, size_t n, cudaStream_t stream);
+
+// Host layout of the tensor-core B operand tiles and centroid norms (table_tc.cu).
+bool make_tc_panels(const std::vector<float>& pivots, const std::vector<int32_t>& chunk_off, int dim,
+                    std::vector<uint8_t>& hi, std::vector<uint8_t>& lo, std::vector<float>& pnorm, int& p_out,
+                    int& groups_out);
+size_t table_tc_smem(int M, int groups);
+
+// BF16 PQ tables of a query batch on the tensor cores (table_tc.cu):
+// tables[q][c][j] = |r_qc|^2 - 2 r_qc . P_cj + |P_cj|^2 with r = q - centroid.
+cudaError_t launch_table_tc(const DeviceIndex& ix, int dim, int M, const float* queries, int nq, int split3,
+                            __nv_bfloat16* tables, cudaStream_t stream);
 
 // Per-warp shared-memory footprint of the plain kernel, in bytes.
 size_t plain_smem_per_warp(int M, int L, int max_m, int k, int dim);
@@ -108,5 +157,10 @@ struct gann_index {
   float* d_dists = nullptr;
   int32_t* d_found = nullptr;
   size_t cap_q = 0, cap_out = 0, cap_dists = 0, cap_found = 0;
+  int32_t* d_kq = nullptr;           // per-query k / L uploaded by the host batch entry
+  int32_t* d_lq = nullptr;
+  size_t cap_kq = 0, cap_lq = 0;
+  __nv_bfloat16* d_tables = nullptr; // BF16 tables of one batch (scratch)
+  size_t cap_tables = 0;
   int fma_table = 1, fma_exact = 1;
 };

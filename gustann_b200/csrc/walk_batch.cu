@@ -1,0 +1,381 @@
+// Batched search kernel: the optimised form of the all-in-GPU path.
+//
+// One CTA of W warps serves one query at a time and pulls the next query from a
+// device counter (persistent grid). Per query: the pivot-graph entry walk
+// (src/impl/nav.cuh:13-135) on warp 0 while the other warps build the PQ table
+// (src/impl/pq.cuh:8-59) in shared memory, FP32 or BF16 (or copy a BF16 table
+// built on the tensor cores for the whole batch); then a beam walk that expands
+// up to W candidates per step, one per warp (src/impl/pure_mem.cuh:243-432
+// expands one):
+//   * a direct-mapped cache of the ids already scored for this query (the
+//     visited filter) skips their code gather and ADC; a cache miss only costs
+//     work, never a wrong list, because merged ids are checked against the list;
+//   * new candidates are merged into the sorted list of L entries by inserting
+//     the survivors only (entries below the list's last key), as in the plain form;
+//   * every expanded node's exact distance goes into the top-k
+//     (src/impl/util.cuh:26-46,116-163).
+// L and k may differ per query.
+#include <climits>
+
+#include "search_common.cuh"
+
+namespace gann {
+namespace {
+
+struct BatchSmem {
+  float* q;
+  void* table;
+  uint32_t* hash;
+  uint32_t *la_id, *lb_id;
+  float *la_d, *lb_d;
+  uint32_t* c_id;  // candidates of the current step (W * max_m)
+  float* c_d;
+  uint32_t* s_id;  // survivors, sorted (W * max_m)
+  float* s_d;
+  int32_t* s_lb;   // insertion points, unsorted then sorted
+  int32_t* s_slb;
+  int32_t* sel_id;  // W
+  float* sel_d;     // W exact distances
+  int32_t* topk_id;
+  float* topk_d;
+  int* ctrl;        // [0] qid, [1] nsel, [2] ncand, [3] entry
+};
+
+struct BatchPlan {
+  size_t off[18];
+  size_t total;
+  __host__ __device__ BatchPlan(int M, int tab_bytes, int H, int L, int max_m, int W, int k, int dim) {
+    const size_t C = (size_t)W * max_m;
+    const size_t sz[18] = {4u * (size_t)dim, (size_t)tab_bytes * M * kPivots, 4u * (size_t)H, 4u * (size_t)L,
+                           4u * (size_t)L, 4u * (size_t)L, 4u * (size_t)L, 4 * C, 4 * C, 4 * C, 4 * C,
+                           4 * C, 4 * C, 4u * W, 4u * W, 4u * (size_t)k, 4u * (size_t)k, 64};
+    size_t o = 0;
+    for (int i = 0; i < 18; i++) {
+      off[i] = o;
+      o = align16(o + sz[i]);
+    }
+    total = o;
+  }
+};
+
+__device__ BatchSmem carve_batch(uint8_t* base, const BatchPlan& pl) {
+  BatchSmem s;
+  s.q = (float*)(base + pl.off[0]);
+  s.table = base + pl.off[1];
+  s.hash = (uint32_t*)(base + pl.off[2]);
+  s.la_id = (uint32_t*)(base + pl.off[3]);
+  s.la_d = (float*)(base + pl.off[4]);
+  s.lb_id = (uint32_t*)(base + pl.off[5]);
+  s.lb_d = (float*)(base + pl.off[6]);
+  s.c_id = (uint32_t*)(base + pl.off[7]);
+  s.c_d = (float*)(base + pl.off[8]);
+  s.s_id = (uint32_t*)(base + pl.off[9]);
+  s.s_d = (float*)(base + pl.off[10]);
+  s.s_lb = (int32_t*)(base + pl.off[11]);
+  s.s_slb = (int32_t*)(base + pl.off[12]);
+  s.sel_id = (int32_t*)(base + pl.off[13]);
+  s.sel_d = (float*)(base + pl.off[14]);
+  s.topk_id = (int32_t*)(base + pl.off[15]);
+  s.topk_d = (float*)(base + pl.off[16]);
+  s.ctrl = (int*)(base + pl.off[17]);
+  return s;
+}
+
+__device__ __forceinline__ uint32_t hash_slot(uint32_t id, int bits) { return (id * 2654435761u) >> (32 - bits); }
+
+// Copy one query's BF16 table (M x 256 x 2 bytes, a multiple of 16) from
+// global memory with 16-byte loads.
+__device__ void copy_table(void* dst, const __nv_bfloat16* src, int bytes, int tid, int nthreads) {
+  const uint4* s = reinterpret_cast<const uint4*>(src);
+  uint4* d = reinterpret_cast<uint4*>(dst);
+  for (int i = tid; i < bytes / 16; i += nthreads) d[i] = __ldg(s + i);
+}
+
+template <class T, class TabT, int W>
+__global__ void __launch_bounds__(W * 32, (W <= 4 ? 8 : 4)) batch_search_kernel(BatchParams p) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  const BatchPlan pl(p.M, (int)sizeof(TabT), 1 << p.hash_bits, p.L_max, p.max_m, W, p.k_max, p.dim);
+  const BatchSmem s = carve_batch(smem, pl);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int dim = p.dim, M = p.M, H = 1 << p.hash_bits;
+  TabT* table = reinterpret_cast<TabT*>(s.table);
+  const NavView nv{p.ix.nav_data, p.ix.nav_graph, p.ix.nav_map, p.nav_n, p.nav_max_m, p.nav_start, dim, p.fma,
+                   p.err};
+  const PqView pv{p.ix.pivots_t, p.ix.centroid, p.ix.chunk_off, M, dim, p.fma};
+
+  for (;;) {
+    if (tid == 0) s.ctrl[0] = atomicAdd(p.next_query, 1);
+    __syncthreads();
+    const int qid = s.ctrl[0];
+    if (qid >= p.nq) break;
+    const int L = p.L_per_q ? min(max(__ldg(p.L_per_q + qid), 1), p.L_max) : p.L_max;
+    const int k = p.k_per_q ? min(max(__ldg(p.k_per_q + qid), 1), p.k_max) : p.k_max;
+    for (int i = tid; i < dim; i += W * 32) s.q[i] = __ldg(p.queries + (size_t)qid * dim + i);
+    for (int i = tid; i < H; i += W * 32) s.hash[i] = 0xffffffffu;
+    __syncthreads();
+    int64_t gathered = 0;  // per-warp share of the algorithmic bytes
+    if (warp == 0) {
+      int64_t u0 = entry_node<T>(p.has_nav, nv, p.medoid, s.q, lane, gathered);
+      if (lane == 0) s.ctrl[3] = (int)u0;
+    }
+    if (p.tables) {  // BF16 tables built for the whole batch on the tensor cores
+      copy_table(s.table, p.tables + (size_t)qid * M * kPivots, M * kPivots * 2, tid, W * 32);
+    } else if (W == 1) {
+      build_table(pv, table, s.q, 0, 1, lane);
+    } else if (warp > 0) {
+      build_table(pv, table, s.q, warp - 1, W - 1, lane);
+    }
+    __syncthreads();
+    restore_query(pv, s.q, tid, W * 32);
+    if (tid == 0) {
+      const int u0 = s.ctrl[3];
+      s.ctrl[1] = u0 >= 0 ? 1 : 0;
+      s.ctrl[2] = 0;
+      s.sel_id[0] = u0;
+      if (u0 >= 0) s.hash[hash_slot((uint32_t)u0, p.hash_bits)] = (uint32_t)u0;
+    }
+    __syncthreads();
+
+    // warp 0 state
+    int sz = 0, found = 0, hops = 0, scan_from = 0;
+    uint32_t* list_id = s.la_id;
+    float* list_d = s.la_d;
+    uint32_t* out_id = s.lb_id;
+    float* out_d = s.lb_d;
+
+    for (;;) {
+      const int nsel = s.ctrl[1];
+      if (nsel == 0) break;
+      // Phase A: warp w expands selected node w.
+      if (warp < nsel) {
+        const int64_t u = s.sel_id[warp];
+        bool ok = u >= 0 && u < p.n;
+        const uint8_t* node = p.ix.pages + (u / p.npp) * kPageSize + (u % p.npp) * p.node_len;
+        int deg = 0;
+        if (ok) {
+          deg = __ldg(reinterpret_cast<const int32_t*>(node + p.data_len));
+          ok = deg >= 0 && deg <= p.max_m;
+        }
+        if (!ok) {
+          if (lane == 0) atomicOr(p.err, (u >= 0 && u < p.n) ? kErrBadDegree : kErrBadId);
+          deg = 0;
+        }
+        const int32_t* edge = reinterpret_cast<const int32_t*>(node + p.data_len + 4);
+        int scored = 0;
+        for (int t = lane; t < deg; t += 32) {
+          const int v = __ldg(edge + t);
+          if ((unsigned)v >= (unsigned)p.n) {
+            atomicOr(p.err, kErrBadId);
+            continue;
+          }
+          const uint32_t old = atomicExch(&s.hash[hash_slot((uint32_t)v, p.hash_bits)], (uint32_t)v);
+          if (old == (uint32_t)v) continue;  // scored before for this query
+          const float d = adc(table, p.ix.codes + (size_t)v * M, M);
+          const int slot = atomicAdd(&s.ctrl[2], 1);
+          s.c_id[slot] = (uint32_t)v;
+          s.c_d[slot] = d;
+          scored++;
+        }
+        const float ed = ok ? warp_exact<T>(s.q, reinterpret_cast<const T*>(node), dim, lane, p.fma) : inf_f();
+        if (lane == 0) s.sel_d[warp] = ed;
+        const int sc = __reduce_add_sync(kFull, scored);
+        gathered += ok ? 4 + 4 * deg + p.data_len + (int64_t)sc * M : 0;
+      }
+      __syncthreads();
+      // Phase B (warp 0): top-k, merge, next selection.
+      if (warp == 0) {
+        for (int w = 0; w < nsel; w++) {
+          if (s.sel_d[w] != inf_f()) topk_push(s.topk_d, s.topk_id, found, k, s.sel_d[w], s.sel_id[w], lane);
+          hops++;
+        }
+        const int nc = s.ctrl[2];
+        const bool full = sz == L;
+        const float tail_d = full ? list_d[L - 1] : 0.0f;
+        const uint32_t tail_id = full ? list_id[L - 1] : 0u;
+        int nsv = 0;
+        for (int base = 0; base < nc; base += 32) {
+          const int t = base + lane;
+          bool keep = false;
+          float d = 0.0f;
+          uint32_t id = 0;
+          int lb = 0;
+          if (t < nc) {
+            d = s.c_d[t];
+            id = s.c_id[t];
+            keep = !full || key_less(d, id, tail_d, tail_id);
+            if (keep) {
+              lb = lower_bound_key(list_d, list_id, 0, sz, d, id);
+              if (lb < sz && ((list_id[lb] ^ id) & kMask) == 0) keep = false;
+            }
+          }
+          const unsigned km = __ballot_sync(kFull, keep);
+          __syncwarp();  // every lane has read its entry before any is overwritten
+          if (keep) {
+            const int slot = nsv + __popc(km & ((1u << lane) - 1));
+            s.c_id[slot] = id;  // compacted in place (slot <= t)
+            s.c_d[slot] = d;
+            s.s_lb[slot] = lb;
+          }
+          nsv += __popc(km);
+          __syncwarp();
+        }
+        // rank-sort the survivors (stable), then drop repeated ids
+        for (int j = lane; j < nsv; j += 32) {
+          const float d = s.c_d[j];
+          const uint32_t id = s.c_id[j];
+          int r = 0;
+          for (int f = 0; f < nsv; f++) {
+            const float fd = s.c_d[f];
+            const uint32_t fi = s.c_id[f];
+            r += key_less(fd, fi, d, id) || (fd == d && ((fi ^ id) & kMask) == 0 && f < j);
+          }
+          s.s_id[r] = id;
+          s.s_d[r] = d;
+          s.s_slb[r] = s.s_lb[j];
+        }
+        __syncwarp();
+        int ns = 0;
+        for (int base = 0; base < nsv; base += 32) {
+          const int j = base + lane;
+          uint32_t id = 0;
+          float d = 0.0f;
+          int lb = 0;
+          bool keep = false;
+          if (j < nsv) {
+            id = s.s_id[j];
+            d = s.s_d[j];
+            lb = s.s_slb[j];
+            keep = j == 0 || ((s.s_id[j - 1] ^ id) & kMask) != 0;
+          }
+          const unsigned km = __ballot_sync(kFull, keep);
+          __syncwarp();
+          if (keep) {
+            const int slot = ns + __popc(km & ((1u << lane) - 1));
+            s.s_id[slot] = id;
+            s.s_d[slot] = d;
+            s.s_slb[slot] = lb;
+          }
+          ns += __popc(km);
+          __syncwarp();
+        }
+        const int nsz = min(sz + ns, L);
+        int first_new = ns ? s.s_slb[0] : INT_MAX;
+        if (ns) {
+          for (int i = lane; i < sz; i += 32) {
+            int lo = 0, hi = ns;
+            while (lo < hi) {
+              const int mid = (lo + hi) >> 1;
+              if (s.s_slb[mid] <= i) lo = mid + 1; else hi = mid;
+            }
+            const int dst = i + lo;
+            if (dst < L) {
+              out_id[dst] = list_id[i];
+              out_d[dst] = list_d[i];
+            }
+          }
+          for (int r = lane; r < ns; r += 32) {
+            const int dst = s.s_slb[r] + r;
+            if (dst < L) {
+              out_id[dst] = s.s_id[r];
+              out_d[dst] = s.s_d[r];
+            }
+          }
+          uint32_t* ti = list_id;
+          float* td = list_d;
+          list_id = out_id;
+          list_d = out_d;
+          out_id = ti;
+          out_d = td;
+        }
+        sz = nsz;
+        __syncwarp();
+        // next selection: the first W unexpanded entries (entries before
+        // scan_from are expanded and did not move unless a survivor landed there)
+        if (first_new < scan_from) scan_from = first_new;
+        int nnext = 0;
+        for (int base = scan_from; base < sz && nnext < W; base += 32) {
+          const int i = base + lane;
+          unsigned um = __ballot_sync(kFull, i < sz && !(list_id[i] & kExpanded));
+          if (base == scan_from && um == 0) scan_from = min(base + 32, sz);
+          while (um && nnext < W) {
+            const int b = __ffs(um) - 1;
+            um &= um - 1;
+            if (lane == 0) {
+              s.sel_id[nnext] = (int32_t)(list_id[base + b] & kMask);
+              list_id[base + b] |= kExpanded;
+            }
+            nnext++;
+          }
+          __syncwarp();
+        }
+        if (lane == 0) {
+          s.ctrl[1] = (hops + nnext > kHopCap) ? 0 : nnext;
+          s.ctrl[2] = 0;
+          if (hops + nnext > kHopCap) atomicOr(p.err, kErrHopCap);
+        }
+      }
+      __syncthreads();
+    }
+    // outputs (warp 0 holds the top-k bookkeeping)
+    if (warp == 0) {
+      const size_t row = (size_t)qid * p.k_max;
+      for (int i = lane; i < p.k_max; i += 32) {
+        p.nns[row + i] = i < found ? s.topk_id[i] : 0;
+        p.dists[row + i] = i < found ? s.topk_d[i] : 0.0f;
+      }
+      if (lane == 0) {
+        p.found[qid] = found;
+        if (p.hops) p.hops[qid] = hops;
+      }
+    }
+    if (p.bytes) {
+      if (lane == 0) atomicAdd(reinterpret_cast<unsigned long long*>(p.bytes + qid), (unsigned long long)gathered);
+    }
+    __syncthreads();
+  }
+}
+
+template <class T, class TabT, int W>
+cudaError_t launch_w(const BatchParams& p, int num_sms, cudaStream_t stream) {
+  const BatchPlan pl(p.M, (int)sizeof(TabT), 1 << p.hash_bits, p.L_max, p.max_m, W, p.k_max, p.dim);
+  const size_t smem = pl.total;
+  if (smem > 227 * 1024) return cudaErrorInvalidConfiguration;
+  auto kern = batch_search_kernel<T, TabT, W>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, W * 32, smem);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  int grid = num_sms * per_sm;
+  if (grid > p.nq) grid = p.nq;
+  kern<<<grid, W * 32, smem, stream>>>(p);
+  return cudaGetLastError();
+}
+
+template <class T, class TabT>
+cudaError_t launch_t(const BatchParams& p, int W, int num_sms, cudaStream_t stream) {
+  switch (W) {
+    case 1: return launch_w<T, TabT, 1>(p, num_sms, stream);
+    case 2: return launch_w<T, TabT, 2>(p, num_sms, stream);
+    case 4: return launch_w<T, TabT, 4>(p, num_sms, stream);
+    case 8: return launch_w<T, TabT, 8>(p, num_sms, stream);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace
+
+size_t batch_smem_bytes(int M, int tab_bytes, int hash_bits, int L_max, int max_m, int W, int k_max, int dim) {
+  return BatchPlan(M, tab_bytes, 1 << hash_bits, L_max, max_m, W, k_max, dim).total;
+}
+
+cudaError_t launch_batch(const BatchParams& p, int dtype, int table_bf16, int W, int num_sms, cudaStream_t stream) {
+  if (dtype == GANN_UINT8)
+    return table_bf16 ? launch_t<uint8_t, __nv_bfloat16>(p, W, num_sms, stream)
+                      : launch_t<uint8_t, float>(p, W, num_sms, stream);
+  return table_bf16 ? launch_t<float, __nv_bfloat16>(p, W, num_sms, stream)
+                    : launch_t<float, float>(p, W, num_sms, stream);
+}
+
+}  // namespace gann

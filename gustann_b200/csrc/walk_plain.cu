@@ -13,58 +13,10 @@
 // SMs), so queries of different length balance across the chip.
 #include <climits>
 
-#include "gann_internal.h"
+#include "search_common.cuh"
 
 namespace gann {
 namespace {
-
-constexpr unsigned kFull = 0xffffffffu;
-constexpr int kNavL = 4;    // nav.cuh:11
-constexpr int kNavR = 28;   // nav.cuh:12
-constexpr int kHopCap = 1 << 20;
-constexpr int kNavIterCap = 1 << 16;
-
-__device__ __forceinline__ float inf_f() { return __int_as_float(0x7f800000); }
-
-template <class T>
-__device__ __forceinline__ float load_elem(const T* p, int i);
-template <>
-__device__ __forceinline__ float load_elem<uint8_t>(const uint8_t* p, int i) {
-  return (float)__ldg(p + i);
-}
-template <>
-__device__ __forceinline__ float load_elem<float>(const float* p, int i) {
-  return __ldg(p + i);
-}
-
-// square_sum_32 (util.cuh:26-46): lane-strided accumulation, then a
-// __shfl_down_sync tree 16,8,4,2,1; lane 0's value is the result.
-template <class T>
-__device__ __forceinline__ float warp_exact(const float* q, const T* v, int dim, int lane, int fma) {
-  float acc = 0.0f;
-  for (int i = lane; i < dim; i += 32) {
-    float d = __fsub_rn(q[i], load_elem<T>(v, i));
-    acc = fma ? __fmaf_rn(d, d, acc) : __fadd_rn(acc, __fmul_rn(d, d));
-  }
-#pragma unroll
-  for (int off = 16; off > 0; off >>= 1) acc = __fadd_rn(acc, __shfl_down_sync(kFull, acc, off));
-  return __shfl_sync(kFull, acc, 0);
-}
-
-// lower_bound on the key (dist, id & 0x7fffffff), util.cuh:166-178.
-__device__ __forceinline__ int lower_bound_key(const float* dist, const uint32_t* id, int l, int r, float d,
-                                               uint32_t x) {
-  x &= kMask;
-  while (l < r) {
-    int mid = (l + r) >> 1;
-    float md = dist[mid];
-    if (md < d || (md == d && (id[mid] & kMask) < x))
-      l = mid + 1;
-    else
-      r = mid;
-  }
-  return l;
-}
 
 struct WarpSmem {
   float* table;       // M x 256
@@ -82,8 +34,6 @@ struct WarpSmem {
   int32_t* topk_id;   // k
   float* topk_d;
 };
-
-__host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 
 // Byte offsets of the arrays above inside one warp's slice (host and device).
 struct SmemPlan {
@@ -123,186 +73,6 @@ __device__ WarpSmem carve(uint8_t* base, int M, int L, int max_m, int k, int dim
   return s;
 }
 
-__device__ __forceinline__ bool key_less(float a, uint32_t ai, float b, uint32_t bi) {
-  return a < b || (a == b && (ai & kMask) < (bi & kMask));
-}
-
-// get_entry_kernel_inner (nav.cuh:13-135) for one query, one slot per lane.
-// Returns the pivot graph's local id, or -1 after setting an error bit.
-template <class T>
-__device__ int nav_entry(const PlainParams& p, const float* q, int lane, int64_t& gathered) {
-  const T* nd = reinterpret_cast<const T*>(p.ix.nav_data);
-  const int dim = p.dim;
-  const int64_t glen = (int64_t)p.nav_n * p.nav_max_m;
-  float d0 = warp_exact<T>(q, nd + (size_t)p.nav_start * dim, dim, lane, p.fma_exact);
-  const int vec_bytes = dim * (int)sizeof(T);
-  gathered += vec_bytes;
-  uint32_t my_id = lane == 0 ? (uint32_t)p.nav_start : 0xffffffffu;  // nav.cuh:50-57
-  float my_d = lane == 0 ? d0 : inf_f();
-  int idx = 0, iters = 0;
-  while (idx != -1) {
-    if (++iters > kNavIterCap) {
-      if (lane == 0) atomicOr(p.err, kErrNavCap);
-      return -1;
-    }
-    uint32_t u = __shfl_sync(kFull, my_id, idx);  // nav.cuh:62-68
-    if (lane == idx) my_id |= kExpanded;
-    // 28 slots of the flat row (nav.cuh:69-72); past the array end reads as -1.
-    int v = -1;
-    if (lane < kNavR) {
-      int64_t e = (int64_t)p.nav_max_m * u + lane;
-      v = e < glen ? __ldg(p.ix.nav_graph + e) : -1;
-    }
-    unsigned neg = __ballot_sync(kFull, lane < kNavR && v == -1);
-    int deg = neg ? __ffs(neg) - 1 : kNavR;
-    // row slots read up to and including the first -1, plus one vector per neighbour
-    gathered += 4 * (deg < kNavR ? deg + 1 : kNavR) + (int64_t)deg * vec_bytes;
-    for (int i = 0; i < deg; i++) {  // nav.cuh:70-81
-      int vi = __shfl_sync(kFull, v, i);
-      if ((unsigned)vi >= (unsigned)p.nav_n) {
-        if (lane == 0) atomicOr(p.err, kErrBadId);
-        return -1;
-      }
-      float di = warp_exact<T>(q, nd + (size_t)vi * dim, dim, lane, p.fma_exact);
-      if (lane == i + kNavL) {
-        my_id = (uint32_t)vi;
-        my_d = di;
-      }
-    }
-#pragma unroll
-    for (int i = 0; i < kNavL; i++) {  // nav.cuh:84-119
-      uint32_t prev = __shfl_sync(kFull, my_id, i > 0 ? i - 1 : 0);
-      float dist = my_d;
-      int pos = lane;
-      bool kill = false;
-      if (lane < i)
-        dist = inf_f();
-      else if (i != 0 && ((my_id ^ prev) & kMask) == 0)
-        kill = true;
-      // Several lanes store prev|own_id to slot i-1 at once in the reference;
-      // the OR of all of them is taken here.
-      unsigned orv = __reduce_or_sync(kFull, kill ? my_id : 0u);
-      unsigned any = __ballot_sync(kFull, kill);
-      if (kill) {
-        dist = inf_f();
-        my_d = inf_f();
-      }
-      if (any && lane == i - 1) my_id = prev | orv;
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) {
-        float od = __shfl_down_sync(kFull, dist, off);
-        int op = __shfl_down_sync(kFull, pos, off);
-        if (od < dist) {
-          dist = od;
-          pos = op;
-        }
-      }
-      int bp = __shfl_sync(kFull, pos, 0);
-      float di = __shfl_sync(kFull, my_d, i), dp = __shfl_sync(kFull, my_d, bp);
-      uint32_t ii = __shfl_sync(kFull, my_id, i), ip = __shfl_sync(kFull, my_id, bp);
-      if (i != bp && di != dp) {
-        if (lane == i) {
-          my_d = dp;
-          my_id = ip;
-        }
-        if (lane == bp) {
-          my_d = di;
-          my_id = ii;
-        }
-      }
-    }
-    unsigned un = __ballot_sync(kFull, !(my_id & kExpanded));  // nav.cuh:120-129
-    int x = un ? __ffs(un) - 1 : 32;
-    idx = x < kNavL ? x : -1;
-  }
-  return (int)(__shfl_sync(kFull, my_id, 0) & kMask);
-}
-
-// PQSearchData::init_query (pq.cuh:8-59): table[c][j] accumulates, over the
-// dimensions i of chunk c in increasing order, (q_i - mu_i - P_t[i][j])^2.
-// Chunks are contiguous ranges, so each (c, j) is accumulated in a register.
-// Afterwards q_i is replaced by fl(fl(q_i - mu_i) + mu_i) (pq.cuh:54-56).
-__device__ void build_table(const PlainParams& p, const WarpSmem& s, int lane) {
-  const int M = p.M;
-  for (int c = 0; c < M; c++) {
-    const int b = __ldg(p.ix.chunk_off + c), e = __ldg(p.ix.chunk_off + c + 1);
-    float acc[8];
-#pragma unroll
-    for (int t = 0; t < 8; t++) acc[t] = 0.0f;
-    for (int i = b; i < e; i++) {
-      const float qc = __fsub_rn(s.q[i], __ldg(p.ix.centroid + i));
-      const float* pt = p.ix.pivots_t + (size_t)i * kPivots + lane;
-#pragma unroll
-      for (int t = 0; t < 8; t++) {
-        float d = __fsub_rn(qc, __ldg(pt + 32 * t));
-        acc[t] = p.fma_table ? __fmaf_rn(d, d, acc[t]) : __fadd_rn(acc[t], __fmul_rn(d, d));
-      }
-    }
-#pragma unroll
-    for (int t = 0; t < 8; t++) s.table[c * kPivots + lane + 32 * t] = acc[t];
-  }
-  __syncwarp();
-  for (int i = lane; i < p.dim; i += 32) {
-    const float mu = __ldg(p.ix.centroid + i);
-    s.q[i] = __fadd_rn(__fsub_rn(s.q[i], mu), mu);
-  }
-  __syncwarp();
-}
-
-// ADC of one code (pure_mem.cuh:302-309): sequential FP32 sum over the chunks.
-__device__ __forceinline__ float adc(const float* table, const uint8_t* code, int M) {
-  float d = 0.0f;
-  if ((M & 15) == 0) {
-    for (int j0 = 0; j0 < M; j0 += 16) {
-      uint4 w = __ldg(reinterpret_cast<const uint4*>(code + j0));
-      uint32_t words[4] = {w.x, w.y, w.z, w.w};
-#pragma unroll
-      for (int b = 0; b < 16; b++) {
-        uint32_t c = (words[b >> 2] >> (8 * (b & 3))) & 0xffu;
-        d = __fadd_rn(d, table[(j0 + b) * kPivots + c]);
-      }
-    }
-  } else {
-    for (int j = 0; j < M; j++) d = __fadd_rn(d, table[j * kPivots + __ldg(code + j)]);
-  }
-  return d;
-}
-
-// retset_push_32 (util.cuh:116-163) by its result: the value goes after every
-// entry with distance <= value; the list keeps at most k entries.
-__device__ void topk_push(float* td, int32_t* ti, int& size, int k, float value, int vid, int lane) {
-  int p = 0;
-  for (int base = 0; base < size; base += 32) {
-    int i = base + lane;
-    p += __popc(__ballot_sync(kFull, i < size && td[i] <= value));
-  }
-  if (p < k) {
-    const int last = size < k ? size : k - 1;  // slot of the last entry after the insert
-    for (int top = last - 1; top >= p; top -= 32) {
-      int i = top - lane;
-      bool act = i >= p;
-      float dv = 0.0f;
-      int32_t iv = 0;
-      if (act) {
-        dv = td[i];
-        iv = ti[i];
-      }
-      __syncwarp();
-      if (act) {
-        td[i + 1] = dv;
-        ti[i + 1] = iv;
-      }
-      __syncwarp();
-    }
-    if (lane == 0) {
-      td[p] = value;
-      ti[p] = vid;
-    }
-  }
-  if (size < k) size++;
-  __syncwarp();
-}
-
 template <class T>
 __device__ void search_query(const PlainParams& p, const WarpSmem& s, int qid, int lane) {
   const int dim = p.dim, L = p.L, k = p.k, max_m = p.max_m, M = p.M;
@@ -310,19 +80,15 @@ __device__ void search_query(const PlainParams& p, const WarpSmem& s, int qid, i
   for (int i = lane; i < dim; i += 32) s.q[i] = __ldg(qg + i);
   __syncwarp();
 
-  int64_t u;
   int64_t gathered = 0;  // algorithmic bytes: records, neighbour ids, codes, pivot vectors
-  if (p.has_nav) {  // pure_mem.cu:106-124
-    int local = nav_entry<T>(p, s.q, lane, gathered);
-    if (local >= p.nav_n) {  // an all-INF slot 0 (fewer than 4 finite candidates)
-      if (lane == 0) atomicOr(p.err, kErrBadId);
-      local = -1;
-    }
-    u = local < 0 ? -2 : (int64_t)__ldg(p.ix.nav_map + local);
-  } else {
-    u = p.medoid;
-  }
-  build_table(p, s, lane);
+  const NavView nv{p.ix.nav_data, p.ix.nav_graph, p.ix.nav_map, p.nav_n, p.nav_max_m, p.nav_start, dim,
+                   p.fma_exact, p.err};
+  int64_t u = entry_node<T>(p.has_nav, nv, p.medoid, s.q, lane, gathered);  // pure_mem.cu:106-124
+  const PqView pv{p.ix.pivots_t, p.ix.centroid, p.ix.chunk_off, M, dim, p.fma_table};
+  build_table(pv, s.table, s.q, 0, 1, lane);
+  __syncwarp();
+  restore_query(pv, s.q, lane, 32);
+  __syncwarp();
 
   int sz = 0, found = 0, hops = 0;
   uint32_t* list_id = s.la_id;

@@ -44,10 +44,19 @@ enum {
 
 /* table precision for gann_search_batch */
 enum {
-  GANN_PREC_FP32 = 0,   /* FP32 tables built on CUDA cores */
-  GANN_PREC_BF16 = 1,   /* BF16 tensor-core table build (FP32 accumulate), BF16 table */
-  GANN_PREC_BF16X3 = 2  /* three-term split-BF16 tensor-core build, BF16 table */
+  GANN_PREC_FP32 = 0,    /* FP32 tables, built per query on CUDA cores (the reference's arithmetic) */
+  GANN_PREC_BF16 = 1,    /* BF16 tables built for the batch on the tensor cores, FP32 accumulate */
+  GANN_PREC_BF16X3 = 2,  /* as BF16, with a three-term split-BF16 product (near-FP32 table values) */
+  GANN_PREC_BF16_CC = 3  /* BF16 tables built per query on CUDA cores (FP32 then rounded) */
 };
+
+/* options of gann_search_batch; zero-initialised = defaults */
+typedef struct {
+  int32_t precision;   /* GANN_PREC_*; default GANN_PREC_BF16 */
+  int32_t beam_width;  /* warps (nodes expanded per step) per query: 1, 2, 4 or 8; 0 = 4 */
+  int32_t hash_bits;   /* visited cache of 2^hash_bits ids per query; 0 = sized from L */
+  int32_t reserved[5];
+} gann_batch_opts_t;
 
 typedef struct {
   int64_t num_points;      /* Layout::num_data   src/layout.hpp:16 */
@@ -110,6 +119,30 @@ int gann_search(gann_t* h, const float* queries, int nq, int topk, int ef_search
 int gann_search_device(gann_t* h, const float* d_queries, int nq, int topk, int ef_search,
                        int32_t* d_nns, float* d_distances, int32_t* d_found_cnt, void* stream);
 
+/*
+ * Batched search (the optimised form): every query has its own topk and
+ * ef_search (arrays of nq, or NULL to use topk_max / ef_max for all), W warps
+ * expand W candidates per step, a visited cache skips already-scored
+ * neighbours, and the PQ tables are BF16 built on the tensor cores (or FP32).
+ * Results are not bit-identical to the reference (that is gann_search); recall
+ * is reported against it. Extends PureMemExecutor::search (src/pure_mem.cu:71-199)
+ * to uneven L and k; the reference asserts one L >= topk per call
+ * (bin/search_disk.cpp:189-192). nns / distances are nq x topk_max (row stride
+ * topk_max); slots past a query's found count hold id 0 and distance 0.
+ */
+int gann_search_batch(gann_t* h, const float* queries, int nq, const int32_t* topk, const int32_t* ef_search,
+                      int topk_max, int ef_max, const gann_batch_opts_t* opts, int32_t* nns,
+                      float* distances, int32_t* found_cnt, double* run_time);
+
+/* gann_search_batch on device buffers (topk / ef_search device arrays or NULL),
+ * enqueued on `stream` (NULL = the handle's stream) without a host
+ * synchronisation; d_hops / d_bytes (nq, may be NULL) receive the per-query
+ * counters of gann_search_device_ex. */
+int gann_search_batch_device(gann_t* h, const float* d_queries, int nq, const int32_t* d_topk,
+                             const int32_t* d_ef_search, int topk_max, int ef_max,
+                             const gann_batch_opts_t* opts, int32_t* d_nns, float* d_distances,
+                             int32_t* d_found_cnt, int32_t* d_hops, int64_t* d_bytes, void* stream);
+
 /* gann_search_device plus per-query counters (device arrays of nq, each may be
  * NULL): d_hops = nodes expanded, d_bytes = algorithmic gathered bytes (degree
  * word, neighbour ids, vector and the codes of every scored neighbour per hop,
@@ -117,6 +150,12 @@ int gann_search_device(gann_t* h, const float* d_queries, int nq, int topk, int 
 int gann_search_device_ex(gann_t* h, const float* d_queries, int nq, int topk, int ef_search,
                           int32_t* d_nns, float* d_distances, int32_t* d_found_cnt, int32_t* d_hops,
                           int64_t* d_bytes, void* stream);
+
+/* PQ distance tables of nq host queries (tables: nq x M x 256 FP32, host),
+ * built as the chosen precision builds them: FP32 exactly as the plain form
+ * (PQSearchData::init_query, src/impl/pq.cuh:8-59); the BF16 forms widened
+ * from their BF16 values. For table-error studies against an FP64 oracle. */
+int gann_pq_tables(gann_t* h, const float* queries, int nq, int precision, float* tables);
 
 /* Synchronise `stream` (NULL = the handle's stream) and report, as
  * GANN_EKERNEL, any error word left by kernels enqueued with

@@ -1,0 +1,150 @@
+"""GPU checks of the batched (optimised) form: PQ-table error of each
+precision against an FP64 oracle, recall against the plain form, uneven L/k,
+and that a query's result is the same alone and inside a mixed batch."""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import gustann_b200 as gb
+from gustann_b200.indexing import build_index, groundtruth, synth
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+def open_meta(meta):
+    g = gb.GustANN(gb.DataType(meta["dtype"]))
+    g.init_pure_mem(gb.GustANNConfig(meta["index_file"], meta["pq_prefix"], meta["nav_dir"] or ""))
+    return g
+
+
+def fp64_tables(meta, q):
+    import struct
+
+    piv = open(meta["pq_prefix"] + "_pivots.bin", "rb").read()
+    nr = struct.unpack_from("<i", piv, 0)[0]
+    offs = np.frombuffer(piv, np.uint64, count=nr, offset=8)
+    dim = q.shape[1]
+    P = np.frombuffer(piv, np.float32, count=256 * dim, offset=int(offs[0]) + 8).reshape(256, dim).astype(np.float64)
+    mu = np.frombuffer(piv, np.float32, count=dim, offset=int(offs[1]) + 8).astype(np.float64)
+    M = meta["M"]
+    co = np.frombuffer(piv, np.uint32, count=M + 1, offset=int(offs[3 if nr == 5 else 2]) + 8)
+    r = q.astype(np.float64) - mu
+    out = np.zeros((q.shape[0], M, 256))
+    for c in range(M):
+        b, e = int(co[c]), int(co[c + 1])
+        out[:, c, :] = ((r[:, None, b:e] - P[None, :, b:e]) ** 2).sum(-1)
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["u8_nav", "f32_nav"])
+def test_table_precision_against_fp64(golden, oracle_mod, name):
+    """FP32 tables equal the reference's (the oracle's) bit for bit; BF16 forms
+    stay within their stated bounds of the FP64 table."""
+    meta = golden[name]
+    g = open_meta(meta)
+    q = meta["queries"][:64]
+    ref = fp64_tables(meta, q)
+    o = oracle_mod.Oracle(meta["index_file"], meta["pq_prefix"], meta["nav_dir"], meta["dtype"])
+    t32 = g.pq_tables(q, gb.PREC_FP32)
+    for i in range(4):
+        np.testing.assert_array_equal(t32[i], o.pq_table(q[i])[0])
+    scale = ref.max(axis=2, keepdims=True)  # per (query, chunk) range of the table
+    err = {}
+    for prec in (gb.PREC_BF16_CC, gb.PREC_BF16X3, gb.PREC_BF16):
+        t = g.pq_tables(q, prec).astype(np.float64)
+        err[prec] = float((np.abs(t - ref) / np.maximum(scale, 1e-30)).max())
+    # BF16 storage: half an ulp of 2^-8 relative; the split product adds ~2^-16
+    assert err[gb.PREC_BF16_CC] <= 2.0 ** -8
+    assert err[gb.PREC_BF16X3] <= 2.0 ** -8 + 2.0 ** -12
+    # single-pass BF16 operands: cancellation in |r|^2 - 2 r.P + |P|^2
+    assert err[gb.PREC_BF16] <= 2.0 ** -5, err
+
+
+@pytest.fixture(scope="module")
+def scale(tmp_path_factory):
+    d = tmp_path_factory.mktemp("bscale")
+    base, qs = synth.make("u8", 200_000, 128, 200, 2000, backend="torch", device="cuda")
+    f = build_index(base, str(d), R=32, M=32, nav_samples=2000, device="cuda")
+    gt = groundtruth.knn(base, qs, 10)
+    g = gb.GustANN(gb.DataType.UINT8)
+    g.init_pure_mem(gb.GustANNConfig(f.index_file, f.pq_prefix, f.nav_dir))
+    return g, qs.float().cpu().numpy(), gt
+
+
+@pytest.mark.gpu
+def test_batch_recall_tracks_plain(scale):
+    g, q, gt = scale
+    for L in (64, 128):
+        plain = groundtruth.recall(g.query(q, 10, L)[0], gt, 10)
+        for prec in (gb.PREC_FP32, gb.PREC_BF16_CC, gb.PREC_BF16X3, gb.PREC_BF16):
+            for W in (1, 4):
+                ids, dis, fnd, t = g.search_batch(q, 10, L, precision=prec, beam_width=W)
+                assert (fnd == 10).all()
+                r = groundtruth.recall(ids, gt, 10)
+                assert r >= plain - 0.03, (L, prec, W, r, plain)
+                assert np.all(np.diff(dis, axis=1) >= 0)
+
+
+@pytest.mark.gpu
+def test_batch_fp32_w1_matches_plain_mostly(scale):
+    """With FP32 tables and one node per step the batched walk differs from the
+    reference walk only by its visited filter; most queries return the same ids."""
+    g, q, gt = scale
+    a = g.query(q, 10, 64)[0]
+    b = g.search_batch(q, 10, 64, precision=gb.PREC_FP32, beam_width=1)[0]
+    same = (a == b).all(1).mean()
+    assert same > 0.8, same
+
+
+@pytest.mark.gpu
+def test_uneven_L_k_and_alone_vs_mixed(scale):
+    g, q, gt = scale
+    q = q[:300]
+    L, k = synth.draws(len(q), [32, 64, 128, 256], [1, 10, 100])
+    for prec, W in ((gb.PREC_BF16, 4), (gb.PREC_FP32, 2)):
+        ids, dis, fnd, _ = g.search_batch(q, k, L, precision=prec, beam_width=W, hash_bits=11)
+        assert ids.shape == (len(q), 100)
+        assert (fnd <= k).all() and (fnd == k).mean() > 0.99
+        for i in range(0, len(q), 37):  # the same query alone, with its own L and k
+            a_ids, a_dis, a_fnd, _ = g.search_batch(q[i:i + 1], int(k[i]), int(L[i]), precision=prec, beam_width=W,
+                                                    hash_bits=11)
+            assert a_fnd[0] == fnd[i]
+            np.testing.assert_array_equal(a_ids[0, :k[i]], ids[i, :k[i]])
+            np.testing.assert_array_equal(a_dis[0, :k[i]], dis[i, :k[i]])
+            assert (ids[i, k[i]:] == 0).all()
+
+
+@pytest.mark.gpu
+def test_batch_device_form_and_counters(scale):
+    import torch
+
+    g, q, gt = scale
+    nq = 500
+    ids, dis, fnd, _ = g.search_batch(q[:nq], 10, 96, precision=gb.PREC_BF16, beam_width=4, hash_bits=10)
+    dq = torch.from_numpy(q[:nq]).cuda()
+    di = torch.zeros((nq, 10), dtype=torch.int32, device="cuda")
+    dd = torch.zeros((nq, 10), dtype=torch.float32, device="cuda")
+    df = torch.zeros(nq, dtype=torch.int32, device="cuda")
+    dh = torch.zeros(nq, dtype=torch.int32, device="cuda")
+    db = torch.zeros(nq, dtype=torch.int64, device="cuda")
+    s = torch.cuda.current_stream().cuda_stream
+    g.search_batch_device(dq.data_ptr(), nq, 0, 0, 10, 96, di.data_ptr(), dd.data_ptr(), df.data_ptr(),
+                          dh.data_ptr(), db.data_ptr(), precision=gb.PREC_BF16, beam_width=4, hash_bits=10, stream=s)
+    g.check(s)
+    np.testing.assert_array_equal(di.cpu().numpy(), ids)
+    np.testing.assert_array_equal(dd.cpu().numpy(), dis)
+    h = dh.cpu().numpy()
+    assert (h >= 96).mean() > 0.9 and (db.cpu().numpy() > 0).all()
+
+
+@pytest.mark.gpu
+def test_batch_argument_errors(scale):
+    g, q, gt = scale
+    with pytest.raises(gb.GustANNError):
+        g.search_batch(q[:4], 10, 64, beam_width=3)
+    with pytest.raises(gb.GustANNError):
+        g.search_batch(q[:4], 10, 64, hash_bits=20)
+    e = g.search_batch(np.zeros((0, 128), np.float32), 10, 64)
+    assert e[0].shape == (0, 10)
