@@ -38,7 +38,7 @@ struct BatchSmem {
   float* sel_d;     // W exact distances
   int32_t* topk_id;
   float* topk_d;
-  int* ctrl;        // [0] qid, [1] nsel, [2] ncand, [3] entry
+  int* ctrl;        // [0] qid, [1] nsel, [2] ncand, [3] entry, [4] survivors, [5] after dedupe
 };
 
 struct BatchPlan {
@@ -136,7 +136,7 @@ __global__ void __launch_bounds__(W * 32, (W <= 4 ? 8 : 4)) batch_search_kernel(
     }
     __syncthreads();
 
-    // warp 0 state
+    // list state (identical in every thread); top-k and selection state (warp 0)
     int sz = 0, found = 0, hops = 0, scan_from = 0;
     uint32_t* list_id = s.la_id;
     float* list_d = s.la_d;
@@ -182,115 +182,121 @@ __global__ void __launch_bounds__(W * 32, (W <= 4 ? 8 : 4)) batch_search_kernel(
         gathered += ok ? 4 + 4 * deg + p.data_len + (int64_t)sc * M : 0;
       }
       __syncthreads();
-      // Phase B (warp 0): top-k, merge, next selection.
+      // Phase B, spread over the CTA: filter the candidates against the list
+      // (B1), rank-sort the survivors (B2), drop repeated ids (B3, rare), move
+      // old entries and survivors into the other list buffer (B4); warp 0 also
+      // keeps the top-k and picks the next nodes (B5).
+      const int nc = s.ctrl[2];
+      const bool full = sz == L;
+      const float tail_d = full ? list_d[L - 1] : 0.0f;
+      const uint32_t tail_id = full ? list_id[L - 1] : 0u;
+      if (tid == 0) s.ctrl[4] = 0;
+      __syncthreads();
+      for (int t = tid; t < nc; t += W * 32) {  // B1
+        const float d = s.c_d[t];
+        const uint32_t id = s.c_id[t];
+        bool keep = !full || key_less(d, id, tail_d, tail_id);
+        int lb = 0;
+        if (keep) {
+          lb = lower_bound_key(list_d, list_id, 0, sz, d, id);
+          if (lb < sz && ((list_id[lb] ^ id) & kMask) == 0) keep = false;
+        }
+        if (keep) {
+          const int slot = atomicAdd(&s.ctrl[4], 1);
+          s.s_id[slot] = id;  // unsorted survivors
+          s.s_d[slot] = d;
+          s.s_lb[slot] = lb;
+        }
+      }
       if (warp == 0) {
         for (int w = 0; w < nsel; w++) {
           if (s.sel_d[w] != inf_f()) topk_push(s.topk_d, s.topk_id, found, k, s.sel_d[w], s.sel_id[w], lane);
           hops++;
         }
-        const int nc = s.ctrl[2];
-        const bool full = sz == L;
-        const float tail_d = full ? list_d[L - 1] : 0.0f;
-        const uint32_t tail_id = full ? list_id[L - 1] : 0u;
-        int nsv = 0;
-        for (int base = 0; base < nc; base += 32) {
-          const int t = base + lane;
-          bool keep = false;
-          float d = 0.0f;
-          uint32_t id = 0;
-          int lb = 0;
-          if (t < nc) {
-            d = s.c_d[t];
-            id = s.c_id[t];
-            keep = !full || key_less(d, id, tail_d, tail_id);
+      }
+      __syncthreads();
+      const int nsv = s.ctrl[4];
+      for (int j = tid; j < nsv; j += W * 32) {  // B2: rank = number of smaller keys (stable)
+        const float d = s.s_d[j];
+        const uint32_t id = s.s_id[j];
+        int r = 0;
+        for (int f = 0; f < nsv; f++) {
+          const float fd = s.s_d[f];
+          const uint32_t fi = s.s_id[f];
+          r += key_less(fd, fi, d, id) || (fd == d && ((fi ^ id) & kMask) == 0 && f < j);
+        }
+        s.c_id[r] = id;
+        s.c_d[r] = d;
+        s.s_slb[r] = s.s_lb[j];
+      }
+      __syncthreads();
+      int ns = nsv;
+      if (warp == 0) {  // B3: the same id twice (a cache eviction between two lookups)
+        bool any = false;
+        for (int j = 1 + lane; j < nsv && !any; j += 32) any = ((s.c_id[j - 1] ^ s.c_id[j]) & kMask) == 0;
+        if (__any_sync(kFull, any)) {
+          int cnt = 0;
+          for (int base = 0; base < nsv; base += 32) {
+            const int j = base + lane;
+            uint32_t id = 0;
+            float d = 0.0f;
+            int lb = 0;
+            bool keep = false;
+            if (j < nsv) {
+              id = s.c_id[j];
+              d = s.c_d[j];
+              lb = s.s_slb[j];
+              keep = j == 0 || ((s.c_id[j - 1] ^ id) & kMask) != 0;
+            }
+            const unsigned km = __ballot_sync(kFull, keep);
+            __syncwarp();
             if (keep) {
-              lb = lower_bound_key(list_d, list_id, 0, sz, d, id);
-              if (lb < sz && ((list_id[lb] ^ id) & kMask) == 0) keep = false;
+              const int slot = cnt + __popc(km & ((1u << lane) - 1));
+              s.c_id[slot] = id;
+              s.c_d[slot] = d;
+              s.s_slb[slot] = lb;
             }
+            cnt += __popc(km);
+            __syncwarp();
           }
-          const unsigned km = __ballot_sync(kFull, keep);
-          __syncwarp();  // every lane has read its entry before any is overwritten
-          if (keep) {
-            const int slot = nsv + __popc(km & ((1u << lane) - 1));
-            s.c_id[slot] = id;  // compacted in place (slot <= t)
-            s.c_d[slot] = d;
-            s.s_lb[slot] = lb;
-          }
-          nsv += __popc(km);
-          __syncwarp();
+          ns = cnt;
         }
-        // rank-sort the survivors (stable), then drop repeated ids
-        for (int j = lane; j < nsv; j += 32) {
-          const float d = s.c_d[j];
-          const uint32_t id = s.c_id[j];
-          int r = 0;
-          for (int f = 0; f < nsv; f++) {
-            const float fd = s.c_d[f];
-            const uint32_t fi = s.c_id[f];
-            r += key_less(fd, fi, d, id) || (fd == d && ((fi ^ id) & kMask) == 0 && f < j);
+        if (lane == 0) s.ctrl[5] = ns;
+      }
+      __syncthreads();
+      ns = s.ctrl[5];
+      const int nsz = min(sz + ns, L);
+      if (ns) {  // B4
+        for (int i = tid; i < sz; i += W * 32) {
+          int lo = 0, hi = ns;  // survivors inserted before old entry i
+          while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (s.s_slb[mid] <= i) lo = mid + 1; else hi = mid;
           }
-          s.s_id[r] = id;
-          s.s_d[r] = d;
-          s.s_slb[r] = s.s_lb[j];
+          const int dst = i + lo;
+          if (dst < L) {
+            out_id[dst] = list_id[i];
+            out_d[dst] = list_d[i];
+          }
         }
-        __syncwarp();
-        int ns = 0;
-        for (int base = 0; base < nsv; base += 32) {
-          const int j = base + lane;
-          uint32_t id = 0;
-          float d = 0.0f;
-          int lb = 0;
-          bool keep = false;
-          if (j < nsv) {
-            id = s.s_id[j];
-            d = s.s_d[j];
-            lb = s.s_slb[j];
-            keep = j == 0 || ((s.s_id[j - 1] ^ id) & kMask) != 0;
+        for (int r = tid; r < ns; r += W * 32) {
+          const int dst = s.s_slb[r] + r;
+          if (dst < L) {
+            out_id[dst] = s.c_id[r];
+            out_d[dst] = s.c_d[r];
           }
-          const unsigned km = __ballot_sync(kFull, keep);
-          __syncwarp();
-          if (keep) {
-            const int slot = ns + __popc(km & ((1u << lane) - 1));
-            s.s_id[slot] = id;
-            s.s_d[slot] = d;
-            s.s_slb[slot] = lb;
-          }
-          ns += __popc(km);
-          __syncwarp();
         }
-        const int nsz = min(sz + ns, L);
-        int first_new = ns ? s.s_slb[0] : INT_MAX;
-        if (ns) {
-          for (int i = lane; i < sz; i += 32) {
-            int lo = 0, hi = ns;
-            while (lo < hi) {
-              const int mid = (lo + hi) >> 1;
-              if (s.s_slb[mid] <= i) lo = mid + 1; else hi = mid;
-            }
-            const int dst = i + lo;
-            if (dst < L) {
-              out_id[dst] = list_id[i];
-              out_d[dst] = list_d[i];
-            }
-          }
-          for (int r = lane; r < ns; r += 32) {
-            const int dst = s.s_slb[r] + r;
-            if (dst < L) {
-              out_id[dst] = s.s_id[r];
-              out_d[dst] = s.s_d[r];
-            }
-          }
-          uint32_t* ti = list_id;
-          float* td = list_d;
-          list_id = out_id;
-          list_d = out_d;
-          out_id = ti;
-          out_d = td;
-        }
-        sz = nsz;
-        __syncwarp();
-        // next selection: the first W unexpanded entries (entries before
-        // scan_from are expanded and did not move unless a survivor landed there)
+        uint32_t* ti = list_id;
+        float* td = list_d;
+        list_id = out_id;
+        list_d = out_d;
+        out_id = ti;
+        out_d = td;
+      }
+      const int first_new = ns ? s.s_slb[0] : INT_MAX;
+      sz = nsz;
+      __syncthreads();
+      if (warp == 0) {  // B5: next selection, the first W unexpanded entries
         if (first_new < scan_from) scan_from = first_new;
         int nnext = 0;
         for (int base = scan_from; base < sz && nnext < W; base += 32) {
