@@ -83,6 +83,76 @@ __device__ BatchSmem carve_batch(uint8_t* base, const BatchPlan& pl) {
 
 __device__ __forceinline__ uint32_t hash_slot(uint32_t id, int bits) { return (id * 2654435761u) >> (32 - bits); }
 
+constexpr int kEdgeRegs = 2;  // neighbour slots held in registers per lane (max_m <= 64 without reloads)
+constexpr int kVecRegs = 4;   // vector elements held in registers per lane (dim <= 128 without reloads)
+
+// ADC with four partial sums (the batched form does not need the reference's
+// summation order; the plain form keeps it).
+template <class TabT>
+__device__ __forceinline__ float adc4(const TabT* table, const uint8_t* code, int M) {
+  if ((M & 15) != 0) return adc(table, code, M);
+  float d0 = 0.0f, d1 = 0.0f, d2 = 0.0f, d3 = 0.0f;
+  for (int j0 = 0; j0 < M; j0 += 16) {
+    const uint4 w = __ldg(reinterpret_cast<const uint4*>(code + j0));
+    const uint32_t words[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+    for (int b = 0; b < 4; b++) {
+      const uint32_t x = words[b];
+      const int base = (j0 + 4 * b) * kPivots;
+      d0 += load_tab(table, base + (x & 0xffu));
+      d1 += load_tab(table, base + kPivots + ((x >> 8) & 0xffu));
+      d2 += load_tab(table, base + 2 * kPivots + ((x >> 16) & 0xffu));
+      d3 += load_tab(table, base + 3 * kPivots + (x >> 24));
+    }
+  }
+  return (d0 + d1) + (d2 + d3);
+}
+
+// Exact squared L2 of the node (its first kVecRegs*32 elements preloaded in
+// vx, lane-strided). uint8 vectors with an integral query are summed in int32
+// (exact); otherwise FP32 with the reference's reduction (util.cuh:26-46).
+template <class T>
+__device__ __forceinline__ float exact_dist(const float* q, const T* v, const float (&vx)[kVecRegs], int dim,
+                                            int lane, bool int_query, int fma) {
+  if (sizeof(T) == 1 && int_query) {
+    int acc = 0;
+#pragma unroll
+    for (int r = 0; r < kVecRegs; r++) {
+      const int i = lane + 32 * r;
+      if (i < dim) {
+        const int d = (int)q[i] - (int)vx[r];
+        acc += d * d;
+      }
+    }
+    for (int i = lane + 32 * kVecRegs; i < dim; i += 32) {
+      const int d = (int)q[i] - (int)load_elem<T>(v, i);
+      acc += d * d;
+    }
+    acc = __reduce_add_sync(kFull, acc);
+    return (float)acc;
+  }
+  float acc = 0.0f;
+#pragma unroll
+  for (int r = 0; r < kVecRegs; r++) {
+    const int i = lane + 32 * r;
+    if (i < dim) {
+      const float d = __fsub_rn(q[i], vx[r]);
+      acc = fma ? __fmaf_rn(d, d, acc) : __fadd_rn(acc, __fmul_rn(d, d));
+    }
+  }
+  for (int i = lane + 32 * kVecRegs; i < dim; i += 32) {
+    const float d = __fsub_rn(q[i], load_elem<T>(v, i));
+    acc = fma ? __fmaf_rn(d, d, acc) : __fadd_rn(acc, __fmul_rn(d, d));
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) acc = __fadd_rn(acc, __shfl_down_sync(kFull, acc, off));
+  return __shfl_sync(kFull, acc, 0);
+}
+
+__device__ __forceinline__ void prefetch_record(const uint8_t* node, int len) {
+  for (int o = 0; o < len; o += 128) asm volatile("prefetch.global.L2 [%0];" ::"l"(node + o));
+}
+
 // Copy one query's BF16 table (M x 256 x 2 bytes, a multiple of 16) from
 // global memory with 16-byte loads.
 __device__ void copy_table(void* dst, const __nv_bfloat16* src, int bytes, int tid, int nthreads) {
@@ -125,8 +195,13 @@ __global__ void __launch_bounds__(W * 32, (W <= 4 ? 8 : 4)) batch_search_kernel(
     } else if (warp > 0) {
       build_table(pv, table, s.q, warp - 1, W - 1, lane);
     }
-    __syncthreads();
-    restore_query(pv, s.q, tid, W * 32);
+    // The exact distances use the query as given (the reference uses
+    // fl(fl(q - mu) + mu), src/impl/pq.cuh:54-56; the batched form does not
+    // reproduce that rounding). uint8 data with integral queries take the
+    // int32 path.
+    bool iq = sizeof(T) == 1;
+    for (int i = tid; i < dim && iq; i += W * 32) iq = s.q[i] == rintf(s.q[i]) && s.q[i] >= 0.0f && s.q[i] <= 255.0f;
+    const bool int_query = __syncthreads_and(iq) != 0;
     if (tid == 0) {
       const int u0 = s.ctrl[3];
       s.ctrl[1] = u0 >= 0 ? 1 : 0;
@@ -146,37 +221,46 @@ __global__ void __launch_bounds__(W * 32, (W <= 4 ? 8 : 4)) batch_search_kernel(
     for (;;) {
       const int nsel = s.ctrl[1];
       if (nsel == 0) break;
-      // Phase A: warp w expands selected node w.
+      // Phase A: warp w expands selected node w. The degree word, the
+      // neighbour slots (up to max_m, inside the record) and the node's vector
+      // are loaded together, so the record costs one memory round trip.
       if (warp < nsel) {
         const int64_t u = s.sel_id[warp];
-        bool ok = u >= 0 && u < p.n;
-        const uint8_t* node = p.ix.pages + (u / p.npp) * kPageSize + (u % p.npp) * p.node_len;
-        int deg = 0;
-        if (ok) {
-          deg = __ldg(reinterpret_cast<const int32_t*>(node + p.data_len));
-          ok = deg >= 0 && deg <= p.max_m;
-        }
+        const bool uok = u >= 0 && u < p.n;
+        const uint8_t* node = p.ix.pages + (uok ? (u / p.npp) * kPageSize + (u % p.npp) * p.node_len : 0);
+        const int32_t* meta = reinterpret_cast<const int32_t*>(node + p.data_len);
+        int deg = __ldg(meta);
+        int ev[kEdgeRegs];
+#pragma unroll
+        for (int r = 0; r < kEdgeRegs; r++) ev[r] = lane + 32 * r < p.max_m ? __ldg(meta + 1 + lane + 32 * r) : -1;
+        float vx[kVecRegs];
+#pragma unroll
+        for (int r = 0; r < kVecRegs; r++) vx[r] = lane + 32 * r < dim ? load_elem<T>(reinterpret_cast<const T*>(node), lane + 32 * r) : 0.0f;
+        const bool ok = uok && deg >= 0 && deg <= p.max_m;
         if (!ok) {
-          if (lane == 0) atomicOr(p.err, (u >= 0 && u < p.n) ? kErrBadDegree : kErrBadId);
+          if (lane == 0) atomicOr(p.err, uok ? kErrBadDegree : kErrBadId);
           deg = 0;
         }
-        const int32_t* edge = reinterpret_cast<const int32_t*>(node + p.data_len + 4);
         int scored = 0;
-        for (int t = lane; t < deg; t += 32) {
-          const int v = __ldg(edge + t);
+        auto score = [&](int v) {
           if ((unsigned)v >= (unsigned)p.n) {
             atomicOr(p.err, kErrBadId);
-            continue;
+            return;
           }
           const uint32_t old = atomicExch(&s.hash[hash_slot((uint32_t)v, p.hash_bits)], (uint32_t)v);
-          if (old == (uint32_t)v) continue;  // scored before for this query
-          const float d = adc(table, p.ix.codes + (size_t)v * M, M);
+          if (old == (uint32_t)v) return;  // scored before for this query
+          const float d = adc4(table, p.ix.codes + (size_t)v * M, M);
           const int slot = atomicAdd(&s.ctrl[2], 1);
           s.c_id[slot] = (uint32_t)v;
           s.c_d[slot] = d;
           scored++;
-        }
-        const float ed = ok ? warp_exact<T>(s.q, reinterpret_cast<const T*>(node), dim, lane, p.fma) : inf_f();
+        };
+#pragma unroll
+        for (int r = 0; r < kEdgeRegs; r++)
+          if (lane + 32 * r < deg) score(ev[r]);
+        for (int t = lane + 32 * kEdgeRegs; t < deg; t += 32) score(__ldg(meta + 1 + t));
+        float ed = inf_f();
+        if (ok) ed = exact_dist<T>(s.q, reinterpret_cast<const T*>(node), vx, dim, lane, int_query, p.fma);
         if (lane == 0) s.sel_d[warp] = ed;
         const int sc = __reduce_add_sync(kFull, scored);
         gathered += ok ? 4 + 4 * deg + p.data_len + (int64_t)sc * M : 0;
@@ -306,10 +390,15 @@ __global__ void __launch_bounds__(W * 32, (W <= 4 ? 8 : 4)) batch_search_kernel(
           while (um && nnext < W) {
             const int b = __ffs(um) - 1;
             um &= um - 1;
+            const uint32_t id = list_id[base + b] & kMask;
             if (lane == 0) {
-              s.sel_id[nnext] = (int32_t)(list_id[base + b] & kMask);
+              s.sel_id[nnext] = (int32_t)id;
               list_id[base + b] |= kExpanded;
             }
+            // start pulling the record toward L2 before the barrier
+            if (lane == nnext && id < (uint32_t)p.n)
+              prefetch_record(p.ix.pages + ((int64_t)id / p.npp) * kPageSize + ((int64_t)id % p.npp) * p.node_len,
+                              (int)p.node_len);
             nnext++;
           }
           __syncwarp();
