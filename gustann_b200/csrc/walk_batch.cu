@@ -8,8 +8,12 @@
 // up to W candidates per step, one per warp (src/impl/pure_mem.cuh:243-432
 // expands one):
 //   * a direct-mapped cache of the ids already scored for this query (the
-//     visited filter) skips their code gather and ADC; a cache miss only costs
-//     work, never a wrong list, because merged ids are checked against the list;
+//     visited filter) skips their code gather and ADC. A hit is always a node
+//     the list has already considered (the entry node is listed as expanded),
+//     and a node the list has considered is rejected when it is scored again:
+//     it is either still in the list (same key) or at or above the list's last
+//     key, which only decreases. So the cache's contents, which depend on the
+//     order of the warps' atomicExch, change the work done but never the result;
 //   * new candidates are merged into the sorted list of L entries by inserting
 //     the survivors only (entries below the list's last key), as in the plain form;
 //   * every expanded node's exact distance goes into the top-k
@@ -25,7 +29,7 @@ namespace {
 struct BatchSmem {
   float* q;
   void* table;
-  uint32_t* hash;
+  uint32_t* hash;   // visited cache: one id per slot
   uint32_t *la_id, *lb_id;
   float *la_d, *lb_d;
   uint32_t* c_id;  // candidates of the current step (W * max_m)
@@ -202,17 +206,25 @@ __global__ void __launch_bounds__(W * 32, (W <= 4 ? 8 : 4)) batch_search_kernel(
     bool iq = sizeof(T) == 1;
     for (int i = tid; i < dim && iq; i += W * 32) iq = s.q[i] == rintf(s.q[i]) && s.q[i] >= 0.0f && s.q[i] <= 255.0f;
     const bool int_query = __syncthreads_and(iq) != 0;
+    // The entry node starts the list as an expanded entry with its ADC
+    // distance (the reference expands it without listing it, pure_mem.cuh:285-
+    // 287). Listing it makes every expanded node one that the list has seen,
+    // so a later re-score of it is rejected whatever the visited cache holds.
+    const int u0 = s.ctrl[3];
     if (tid == 0) {
-      const int u0 = s.ctrl[3];
       s.ctrl[1] = u0 >= 0 ? 1 : 0;
       s.ctrl[2] = 0;
       s.sel_id[0] = u0;
-      if (u0 >= 0) s.hash[hash_slot((uint32_t)u0, p.hash_bits)] = (uint32_t)u0;
+      if (u0 >= 0) {
+        s.hash[hash_slot((uint32_t)u0, p.hash_bits)] = (uint32_t)u0;
+        s.la_id[0] = (uint32_t)u0 | kExpanded;
+        s.la_d[0] = adc4(table, p.ix.codes + (size_t)u0 * M, M);
+      }
     }
     __syncthreads();
 
     // list state (identical in every thread); top-k and selection state (warp 0)
-    int sz = 0, found = 0, hops = 0, scan_from = 0;
+    int sz = u0 >= 0 ? 1 : 0, found = 0, hops = 0, scan_from = 0;
     uint32_t* list_id = s.la_id;
     float* list_d = s.la_d;
     uint32_t* out_id = s.lb_id;

@@ -148,3 +148,16 @@ def test_batch_argument_errors(scale):
         g.search_batch(q[:4], 10, 64, hash_bits=20)
     e = g.search_batch(np.zeros((0, 128), np.float32), 10, 64)
     assert e[0].shape == (0, 10)
+
+
+@pytest.mark.gpu
+def test_batch_is_deterministic(scale):
+    """Two runs of the same batch give bit-identical ids and distances (the
+    visited cache's state does not depend on warp timing)."""
+    g, q, gt = scale
+    for prec, L, hb in ((gb.PREC_FP32, 48, 6), (gb.PREC_BF16, 64, 7), (gb.PREC_BF16, 256, 0)):
+        a = g.search_batch(q, 10, L, precision=prec, beam_width=4, hash_bits=hb)
+        for _ in range(2):
+            b = g.search_batch(q, 10, L, precision=prec, beam_width=4, hash_bits=hb)
+            np.testing.assert_array_equal(a[0], b[0])
+            np.testing.assert_array_equal(a[1].view(np.uint32), b[1].view(np.uint32))
