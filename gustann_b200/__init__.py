@@ -85,6 +85,7 @@ _SIGNATURES = {
     "gann_search_device_ex": (_I, [_P, _P, _I, _I, _I, _P, _P, _P, _P, _P, _P]),
     "gann_search_batch": (_I, [_P, _P, _I, _P, _P, _I, _I, _P, _P, _P, _P, ctypes.POINTER(ctypes.c_double)]),
     "gann_search_batch_device": (_I, [_P, _P, _I, _P, _P, _I, _I, _P, _P, _P, _P, _P, _P, _P]),
+    "gann_search_batch_noalloc": (_I, [_P, _P, _I, _I, _I, _P, _P, _P, _P, _P]),
     "gann_pq_tables": (_I, [_P, _P, _I, _I, _P]),
     "gann_check": (_I, [_P, _P]),
     "gann_set_fma": (_I, [_P, _I, _I]),

@@ -190,6 +190,9 @@ int kernel_error_status(unsigned int err) {
 
 }  // namespace
 
+// Message slot of gann_last_error() for entry points defined in other files.
+int gann_internal_set_error(int code, const char* msg) { return set_error(code, msg); }
+
 extern "C" {
 
 const char* gann_last_error(void) { return g_last_error.c_str(); }

@@ -151,6 +151,27 @@ int gann_search_device_ex(gann_t* h, const float* d_queries, int nq, int topk, i
                           int32_t* d_nns, float* d_distances, int32_t* d_found_cnt, int32_t* d_hops,
                           int64_t* d_bytes, void* stream);
 
+/*
+ * gann_search_batch_device for callers that cannot allocate device memory
+ * while they search: a serving loop that must not stall on cudaMalloc (which
+ * can synchronise the device and takes the driver's allocation lock), or a
+ * host program whose memory manager owns every device allocation after
+ * start-up. No counterpart in the reference (its search allocates device
+ * vectors on every call, src/pure_mem.cu:78-89).
+ * Same arguments as gann_search_batch_device with one topk / ef_search for the
+ * whole call; no per-query counters. The call allocates nothing: its scratch
+ * (work counter, BF16 tables) is a fixed 8 MiB + 256 B array inside the
+ * library, held on every GPU that loads libgann until the process exits.
+ * Limits: nq <= 512 per call and, for tensor-core tables, at most 32 PQ
+ * chunks; larger requests return GANN_ERANGE. All calls on a device share the
+ * array: calls whose work overlaps on the GPU race on it and must be
+ * serialised by the caller. The first call on a device looks up the array's
+ * device address; make it before any stream capture.
+ */
+int gann_search_batch_noalloc(gann_t* h, const float* d_queries, int nq, int topk, int ef_search,
+                              const gann_batch_opts_t* opts, int32_t* d_nns, float* d_distances,
+                              int32_t* d_found_cnt, void* stream);
+
 /* PQ distance tables of nq host queries (tables: nq x M x 256 FP32, host),
  * built as the chosen precision builds them: FP32 exactly as the plain form
  * (PQSearchData::init_query, src/impl/pq.cuh:8-59); the BF16 forms widened
