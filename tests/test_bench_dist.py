@@ -1,0 +1,68 @@
+"""bench.py's multi-rank plumbing on CPU: world size 2 over gloo. Each rank
+times its own replica; the reported time is the max over ranks; ranks that do
+not build the index wait for the builder's ready file; the reference arm runs
+on rank 0 only."""
+import json
+import os
+import socket
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import pytest
+import torch.multiprocessing as mp
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _worker(rank, world, port, tmp, results):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world),
+                      LOCAL_RANK=str(rank))
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    dist = bench.init_dist(world, "gloo")
+    ready = Path(tmp) / "ready.json"
+    if rank == 0:
+        time.sleep(0.5)
+        ready.write_text("{}")
+    else:
+        bench.wait_for(ready, 30)
+    bench.barrier(world)
+    t = bench.max_over_ranks(10.0 * (rank + 1), world)
+    results[rank] = t
+    dist.destroy_process_group()
+
+
+@pytest.mark.timeout(120)
+def test_max_over_ranks_and_ready_file_gloo():
+    world = 2
+    with tempfile.TemporaryDirectory() as tmp:
+        mgr = mp.Manager()
+        results = mgr.dict()
+        mp.start_processes(_worker, args=(world, _free_port(), tmp, results), nprocs=world, start_method="spawn")
+        assert dict(results) == {0: 20.0, 1: 20.0}
+
+
+def test_single_rank_helpers_are_identity():
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    assert bench.max_over_ranks(3.5, 1) == 3.5
+    bench.barrier(1)
+    assert bench.dist_env()[1] >= 1
+
+
+def test_wait_for_times_out(tmp_path):
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    with pytest.raises(TimeoutError):
+        bench.wait_for(tmp_path / "never", 0.1)
