@@ -252,21 +252,41 @@ class BatchRunner(PlainRunner):
 
 
 def calibrate(runner, gt, k, target, fixed_L=None):
+    """Smallest L (to a step of 8) whose recall@k reaches the target: walk the
+    ladder, then bisect between the last ladder value that missed and the first
+    that reached it."""
     import torch
 
-    ladder = [fixed_L] if fixed_L else L_LADDER
-    best = None
-    for L in ladder:
-        if L < k:
-            continue
+    def recall_for(L):
         runner.run(L)
         torch.cuda.synchronize()
         runner.g.check()
-        r = recall_at(runner.ids.cpu().numpy(), gt, k)
+        return recall_at(runner.ids.cpu().numpy(), gt, k)
+
+    if fixed_L:
+        return fixed_L, recall_for(fixed_L)
+    lo, best = None, None
+    for L in L_LADDER:
+        if L < k:
+            continue
+        r = recall_for(L)
         best = (L, r)
         if r >= target:
             break
-    return best
+        lo = L
+    if best is None or best[1] < target or lo is None:
+        return best
+    hi = best
+    while hi[0] - lo > 8:
+        mid = (lo + hi[0]) // 2 // 8 * 8
+        if mid <= lo:
+            break
+        r = recall_for(mid)
+        if r >= target:
+            hi = (mid, r)
+        else:
+            lo = mid
+    return hi
 
 
 def time_steps(runner, L, steps, warmup, world, flush):
@@ -345,12 +365,14 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def traffic_per_query(kernel: str, workload: str):
-    """DRAM bytes per query of `kernel` from a committed ncu summary, if any."""
+def traffic_per_hop(kernel: str, workload: str):
+    """DRAM bytes per hop of `kernel` from a committed ncu capture of the same
+    workload (profiles/<kernel>_<workload>.json), if any. The bench scales it by
+    the hops it counted, since its calibrated L may differ from the capture's."""
     p = ROOT / "profiles" / f"{kernel}_{workload}.json"
     if p.exists():
         d = json.loads(p.read_text())
-        return d.get("dram_bytes_per_query")
+        return d.get("dram_bytes_per_hop")
     return None
 
 
@@ -411,7 +433,7 @@ def _run_ours(args, rank, world, local):
     nq = runner.nq
     peak, peak_kind = load_peaks()
     achieved = r["bytes_per_step"] / (r["avg_ms"] / 1e3) / 1e9
-    tpq = traffic_per_query("batch_search_kernel" if head != "plain" else "plain_search_kernel", args.workload)
+    tph = traffic_per_hop("batch_search_kernel" if head != "plain" else "plain_search_kernel", args.workload)
     qp = torch.from_numpy(meta["queries"]).pin_memory()
     e2e_val, h2d, d2h = e2e_steps(runner, qp, r["L"], max(2, min(args.steps, 5)), 1)
     e2e_total = max_over_ranks(1.0 / e2e_val, world, device="cuda")
@@ -430,7 +452,9 @@ def _run_ours(args, rank, world, local):
         "gathered_bytes_per_query": r["bytes_per_step"] / nq,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak if peak else None,
-                     "traffic": None if tpq is None else tpq * nq, "peak_kind": peak_kind,
+                     "traffic": None if tph is None else tph * r["hops_per_query"] * nq,
+                     "traffic_source": "ncu capture scaled by counted hops (profiles/)" if tph else None,
+                     "peak_kind": peak_kind,
                      "kernel": "batch_search_kernel" if head != "plain" else "plain_search_kernel"},
         "e2e": {"value": world / e2e_total, "unit": "queries/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
