@@ -32,9 +32,9 @@ struct BatchSmem {
   uint32_t* hash;   // visited cache: one id per slot
   uint32_t *la_id, *lb_id;
   float *la_d, *lb_d;
-  uint32_t* c_id;  // candidates of the current step (W * max_m)
-  float* c_d;
-  uint32_t* s_id;  // survivors, sorted (W * max_m)
+  uint32_t* c_id;  // [0, W): list positions of the picks; then the sorted survivors (W * max_m)
+  float* c_d;      // sorted survivor distances
+  uint32_t* s_id;  // survivors of the step, unsorted (W * max_m)
   float* s_d;
   int32_t* s_lb;   // insertion points, unsorted then sorted
   int32_t* s_slb;
@@ -42,19 +42,20 @@ struct BatchSmem {
   float* sel_d;     // W exact distances
   int32_t* topk_id;
   float* topk_d;
-  int* ctrl;        // [0] qid, [1] nsel, [2] ncand, [3] entry, [4] survivors, [5] after dedupe
+  int* ctrl;        // [0] qid, [2] survivors, [3] entry, [4] repeated id, [5] after dedupe, [6] stop
+  uint32_t* wnew;   // W * max_m: per-warp list of newly seen neighbours
 };
 
 struct BatchPlan {
-  size_t off[18];
+  size_t off[19];
   size_t total;
   __host__ __device__ BatchPlan(int M, int tab_bytes, int H, int L, int max_m, int W, int k, int dim) {
     const size_t C = (size_t)W * max_m;
-    const size_t sz[18] = {4u * (size_t)dim, (size_t)tab_bytes * M * kPivots, 4u * (size_t)H, 4u * (size_t)L,
-                           4u * (size_t)L, 4u * (size_t)L, 4u * (size_t)L, 4 * C, 4 * C, 4 * C, 4 * C,
-                           4 * C, 4 * C, 4u * W, 4u * W, 4u * (size_t)k, 4u * (size_t)k, 64};
+    const size_t sz[19] = {4u * (size_t)dim, (size_t)tab_bytes * M * kPivots, 4u * (size_t)H, 4u * (size_t)L,
+                           4u * (size_t)L, 4u * (size_t)L, 4u * (size_t)L, 4 * (C + W), 4 * C, 4 * C, 4 * C,
+                           4 * C, 4 * C, 4u * W, 4u * W, 4u * (size_t)k, 4u * (size_t)k, 64, 4 * C};
     size_t o = 0;
-    for (int i = 0; i < 18; i++) {
+    for (int i = 0; i < 19; i++) {
       off[i] = o;
       o = align16(o + sz[i]);
     }
@@ -82,6 +83,7 @@ __device__ BatchSmem carve_batch(uint8_t* base, const BatchPlan& pl) {
   s.topk_id = (int32_t*)(base + pl.off[15]);
   s.topk_d = (float*)(base + pl.off[16]);
   s.ctrl = (int*)(base + pl.off[17]);
+  s.wnew = (uint32_t*)(base + pl.off[18]);
   return s;
 }
 
@@ -90,26 +92,31 @@ __device__ __forceinline__ uint32_t hash_slot(uint32_t id, int bits) { return (i
 constexpr int kEdgeRegs = 2;  // neighbour slots held in registers per lane (max_m <= 64 without reloads)
 constexpr int kVecRegs = 4;   // vector elements held in registers per lane (dim <= 128 without reloads)
 
-// ADC with four partial sums (the batched form does not need the reference's
-// summation order; the plain form keeps it).
+// ADC of the batched form. For M a multiple of 16 the chunks are split into
+// four contiguous quarters summed in chunk order, four accumulators in flight,
+// and the result is (q0 + q1) + (q2 + q3); every score of a node (the entry
+// included) uses this function, so a re-score reproduces the same key. Other
+// M: a sequential sum (the plain form's adc).
 template <class TabT>
-__device__ __forceinline__ float adc4(const TabT* table, const uint8_t* code, int M) {
-  if ((M & 15) != 0) return adc(table, code, M);
-  float d0 = 0.0f, d1 = 0.0f, d2 = 0.0f, d3 = 0.0f;
-  for (int j0 = 0; j0 < M; j0 += 16) {
-    const uint4 w = __ldg(reinterpret_cast<const uint4*>(code + j0));
-    const uint32_t words[4] = {w.x, w.y, w.z, w.w};
-#pragma unroll
-    for (int b = 0; b < 4; b++) {
-      const uint32_t x = words[b];
-      const int base = (j0 + 4 * b) * kPivots;
-      d0 += load_tab(table, base + (x & 0xffu));
-      d1 += load_tab(table, base + kPivots + ((x >> 8) & 0xffu));
-      d2 += load_tab(table, base + 2 * kPivots + ((x >> 16) & 0xffu));
-      d3 += load_tab(table, base + 3 * kPivots + (x >> 24));
-    }
+__device__ __forceinline__ float quarter_sum(const TabT* table, const uint8_t* code, int c0, int nc) {
+  float d = 0.0f;
+  for (int w = 0; w < nc; w += 4) {
+    const uint32_t x = __ldg(reinterpret_cast<const uint32_t*>(code + c0 + w));
+    d += load_tab(table, (c0 + w) * kPivots + (x & 0xffu));
+    d += load_tab(table, (c0 + w + 1) * kPivots + ((x >> 8) & 0xffu));
+    d += load_tab(table, (c0 + w + 2) * kPivots + ((x >> 16) & 0xffu));
+    d += load_tab(table, (c0 + w + 3) * kPivots + (x >> 24));
   }
-  return (d0 + d1) + (d2 + d3);
+  return d;
+}
+
+template <class TabT>
+__device__ __forceinline__ float adc_split4(const TabT* table, const uint8_t* code, int M) {
+  if ((M & 15) != 0) return adc(table, code, M);
+  const int q = M >> 2;
+  const float s0 = quarter_sum(table, code, 0, q), s1 = quarter_sum(table, code, q, q);
+  const float s2 = quarter_sum(table, code, 2 * q, q), s3 = quarter_sum(table, code, 3 * q, q);
+  return (s0 + s1) + (s2 + s3);
 }
 
 // Exact squared L2 of the node (its first kVecRegs*32 elements preloaded in
@@ -206,24 +213,25 @@ __global__ void __launch_bounds__(W * 32, (W <= 4 ? 8 : 4)) batch_search_kernel(
     bool iq = sizeof(T) == 1;
     for (int i = tid; i < dim && iq; i += W * 32) iq = s.q[i] == rintf(s.q[i]) && s.q[i] >= 0.0f && s.q[i] <= 255.0f;
     const bool int_query = __syncthreads_and(iq) != 0;
-    // The entry node starts the list as an expanded entry with its ADC
-    // distance (the reference expands it without listing it, pure_mem.cuh:285-
-    // 287). Listing it makes every expanded node one that the list has seen,
-    // so a later re-score of it is rejected whatever the visited cache holds.
+    // The entry node starts the list, unexpanded, with its ADC distance; the
+    // first step picks it (the reference expands it without listing it,
+    // src/impl/pure_mem.cuh:285-287). Listing it makes every expanded node one
+    // that the list has seen, so a later re-score of it is rejected whatever
+    // the visited cache holds.
     const int u0 = s.ctrl[3];
     if (tid == 0) {
-      s.ctrl[1] = u0 >= 0 ? 1 : 0;
-      s.ctrl[2] = 0;
-      s.sel_id[0] = u0;
+      s.ctrl[2] = 0;  // survivors of the current step
+      s.ctrl[4] = 0;  // a repeated id among them
+      s.ctrl[6] = 0;  // stop (hop limit)
       if (u0 >= 0) {
         s.hash[hash_slot((uint32_t)u0, p.hash_bits)] = (uint32_t)u0;
-        s.la_id[0] = (uint32_t)u0 | kExpanded;
-        s.la_d[0] = adc4(table, p.ix.codes + (size_t)u0 * M, M);
+        s.la_id[0] = (uint32_t)u0;
+        s.la_d[0] = adc_split4(table, p.ix.codes + (size_t)u0 * M, M);
       }
     }
     __syncthreads();
 
-    // list state (identical in every thread); top-k and selection state (warp 0)
+    // List state, identical in every thread; top-k state in warp 0.
     int sz = u0 >= 0 ? 1 : 0, found = 0, hops = 0, scan_from = 0;
     uint32_t* list_id = s.la_id;
     float* list_d = s.la_d;
@@ -231,14 +239,32 @@ __global__ void __launch_bounds__(W * 32, (W <= 4 ? 8 : 4)) batch_search_kernel(
     float* out_d = s.lb_d;
 
     for (;;) {
-      const int nsel = s.ctrl[1];
-      if (nsel == 0) break;
-      // Phase A: warp w expands selected node w. The degree word, the
-      // neighbour slots (up to max_m, inside the record) and the node's vector
-      // are loaded together, so the record costs one memory round trip.
-      if (warp < nsel) {
-        const int64_t u = s.sel_id[warp];
-        const bool uok = u >= 0 && u < p.n;
+      // Pick: every warp finds the same first W unexpanded entries (entries
+      // before scan_from are expanded and have not moved) and takes its own.
+      int npick = 0, my_pos = -1;
+      for (int base = scan_from; base < sz && npick < W; base += 32) {
+        const int i = base + lane;
+        unsigned um = __ballot_sync(kFull, i < sz && !(list_id[i] & kExpanded));
+        if (base == scan_from && um == 0) scan_from = min(base + 32, sz);
+        while (um && npick < W) {
+          const int b = __ffs(um) - 1;
+          um &= um - 1;
+          if (npick == warp) my_pos = base + b;
+          npick++;
+        }
+      }
+      if (npick == 0 || s.ctrl[6]) break;
+      const bool full = sz == L;
+      const float tail_d = full ? list_d[L - 1] : 0.0f;
+      const uint32_t tail_id = full ? list_id[L - 1] : 0u;
+      // Expand: warp w expands pick w. The degree word, the neighbour slots
+      // (up to max_m, inside the record) and the node's vector are loaded
+      // together, so the record costs one memory round trip. New neighbours
+      // are scored and checked against the list here; survivors (below the
+      // list's last key when it is full, not in it yet) are kept unsorted.
+      if (warp < npick) {
+        const int64_t u = list_id[my_pos] & kMask;
+        const bool uok = u < p.n;
         const uint8_t* node = p.ix.pages + (uok ? (u / p.npp) * kPageSize + (u % p.npp) * p.node_len : 0);
         const int32_t* meta = reinterpret_cast<const int32_t*>(node + p.data_len);
         int deg = __ldg(meta);
@@ -247,90 +273,100 @@ __global__ void __launch_bounds__(W * 32, (W <= 4 ? 8 : 4)) batch_search_kernel(
         for (int r = 0; r < kEdgeRegs; r++) ev[r] = lane + 32 * r < p.max_m ? __ldg(meta + 1 + lane + 32 * r) : -1;
         float vx[kVecRegs];
 #pragma unroll
-        for (int r = 0; r < kVecRegs; r++) vx[r] = lane + 32 * r < dim ? load_elem<T>(reinterpret_cast<const T*>(node), lane + 32 * r) : 0.0f;
+        for (int r = 0; r < kVecRegs; r++)
+          vx[r] = lane + 32 * r < dim ? load_elem<T>(reinterpret_cast<const T*>(node), lane + 32 * r) : 0.0f;
         const bool ok = uok && deg >= 0 && deg <= p.max_m;
         if (!ok) {
           if (lane == 0) atomicOr(p.err, uok ? kErrBadDegree : kErrBadId);
           deg = 0;
         }
-        int scored = 0;
-        auto score = [&](int v) {
-          if ((unsigned)v >= (unsigned)p.n) {
-            atomicOr(p.err, kErrBadId);
-            return;
+        // Visited-cache check of every neighbour; the new ones are compacted
+        // into this warp's scratch list.
+        uint32_t* wnew = s.wnew + warp * p.max_m;
+        int nnew = 0;
+        auto check = [&](int t, int v) {
+          bool fresh = false;
+          if (t < deg) {
+            if ((unsigned)v >= (unsigned)p.n)
+              atomicOr(p.err, kErrBadId);
+            else
+              fresh = atomicExch(&s.hash[hash_slot((uint32_t)v, p.hash_bits)], (uint32_t)v) != (uint32_t)v;
           }
-          const uint32_t old = atomicExch(&s.hash[hash_slot((uint32_t)v, p.hash_bits)], (uint32_t)v);
-          if (old == (uint32_t)v) return;  // scored before for this query
-          const float d = adc4(table, p.ix.codes + (size_t)v * M, M);
-          const int slot = atomicAdd(&s.ctrl[2], 1);
-          s.c_id[slot] = (uint32_t)v;
-          s.c_d[slot] = d;
-          scored++;
+          const unsigned m = __ballot_sync(kFull, fresh);
+          if (fresh) wnew[nnew + __popc(m & ((1u << lane) - 1))] = (uint32_t)v;
+          nnew += __popc(m);
         };
 #pragma unroll
-        for (int r = 0; r < kEdgeRegs; r++)
-          if (lane + 32 * r < deg) score(ev[r]);
-        for (int t = lane + 32 * kEdgeRegs; t < deg; t += 32) score(__ldg(meta + 1 + t));
+        for (int r = 0; r < kEdgeRegs; r++) check(lane + 32 * r, ev[r]);
+        for (int b0 = 32 * kEdgeRegs; b0 < deg; b0 += 32)
+          check(b0 + lane, b0 + lane < deg ? __ldg(meta + 1 + b0 + lane) : -1);
+        __syncwarp();
+        // Score the new ones and keep the survivors: below the list's last key
+        // when it is full, not in it yet.
+        auto keep = [&](uint32_t v, float d) {
+          if (full && !key_less(d, v, tail_d, tail_id)) return;
+          const int lb = lower_bound_key(list_d, list_id, 0, sz, d, v);
+          if (lb < sz && ((list_id[lb] ^ v) & kMask) == 0) return;
+          const int slot = atomicAdd(&s.ctrl[2], 1);
+          s.s_id[slot] = v;
+          s.s_d[slot] = d;
+          s.s_lb[slot] = lb;
+        };
+        // One lane per new neighbour: all of the warp's code fetches are in
+        // flight at once, and no lane runs a second ADC while others idle.
+        for (int i = lane; i < nnew; i += 32) {
+          const uint32_t v = wnew[i];
+          keep(v, adc_split4(table, p.ix.codes + (size_t)v * M, M));
+        }
+        const int scored = lane == 0 ? nnew : 0;
         float ed = inf_f();
         if (ok) ed = exact_dist<T>(s.q, reinterpret_cast<const T*>(node), vx, dim, lane, int_query, p.fma);
-        if (lane == 0) s.sel_d[warp] = ed;
+        if (lane == 0) {
+          s.sel_d[warp] = ed;
+          s.sel_id[warp] = (int32_t)u;
+          s.c_id[warp] = (uint32_t)my_pos;  // list position of the pick (marked below)
+        }
         const int sc = __reduce_add_sync(kFull, scored);
         gathered += ok ? 4 + 4 * deg + p.data_len + (int64_t)sc * M : 0;
       }
-      __syncthreads();
-      // Phase B, spread over the CTA: filter the candidates against the list
-      // (B1), rank-sort the survivors (B2), drop repeated ids (B3, rare), move
-      // old entries and survivors into the other list buffer (B4); warp 0 also
-      // keeps the top-k and picks the next nodes (B5).
-      const int nc = s.ctrl[2];
-      const bool full = sz == L;
-      const float tail_d = full ? list_d[L - 1] : 0.0f;
-      const uint32_t tail_id = full ? list_id[L - 1] : 0u;
-      if (tid == 0) s.ctrl[4] = 0;
-      __syncthreads();
-      for (int t = tid; t < nc; t += W * 32) {  // B1
-        const float d = s.c_d[t];
-        const uint32_t id = s.c_id[t];
-        bool keep = !full || key_less(d, id, tail_d, tail_id);
-        int lb = 0;
-        if (keep) {
-          lb = lower_bound_key(list_d, list_id, 0, sz, d, id);
-          if (lb < sz && ((list_id[lb] ^ id) & kMask) == 0) keep = false;
-        }
-        if (keep) {
-          const int slot = atomicAdd(&s.ctrl[4], 1);
-          s.s_id[slot] = id;  // unsorted survivors
-          s.s_d[slot] = d;
-          s.s_lb[slot] = lb;
-        }
-      }
-      if (warp == 0) {
-        for (int w = 0; w < nsel; w++) {
+      __syncthreads();  // (1) survivors and picks are in
+      const int nsv = s.ctrl[2];
+      if (warp == 0) {  // mark the picks, keep the top-k
+        for (int w = 0; w < npick; w++) {
+          if (lane == 0) list_id[s.c_id[w]] |= kExpanded;
           if (s.sel_d[w] != inf_f()) topk_push(s.topk_d, s.topk_id, found, k, s.sel_d[w], s.sel_id[w], lane);
           hops++;
         }
+        if (lane == 0 && hops > kHopCap) {
+          s.ctrl[6] = 1;
+          atomicOr(p.err, kErrHopCap);
+        }
       }
-      __syncthreads();
-      const int nsv = s.ctrl[4];
-      for (int j = tid; j < nsv; j += W * 32) {  // B2: rank = number of smaller keys (stable)
+      // Rank-sort the survivors (rank = number of smaller keys, ties by slot);
+      // a repeated id (a cache eviction between two lookups) raises a flag.
+      for (int j = tid; j < nsv; j += W * 32) {
         const float d = s.s_d[j];
         const uint32_t id = s.s_id[j];
         int r = 0;
+        bool rep = false;
         for (int f = 0; f < nsv; f++) {
           const float fd = s.s_d[f];
           const uint32_t fi = s.s_id[f];
-          r += key_less(fd, fi, d, id) || (fd == d && ((fi ^ id) & kMask) == 0 && f < j);
+          const bool same = fd == d && ((fi ^ id) & kMask) == 0;
+          r += key_less(fd, fi, d, id) || (same && f < j);
+          rep |= same && f != j;
         }
-        s.c_id[r] = id;
+        s.c_id[W + r] = id;  // sorted survivors after the W pick slots
         s.c_d[r] = d;
         s.s_slb[r] = s.s_lb[j];
+        if (rep) s.ctrl[4] = 1;
       }
-      __syncthreads();
+      __syncthreads();  // (2)
+      uint32_t* sid = s.c_id + W;
       int ns = nsv;
-      if (warp == 0) {  // B3: the same id twice (a cache eviction between two lookups)
-        bool any = false;
-        for (int j = 1 + lane; j < nsv && !any; j += 32) any = ((s.c_id[j - 1] ^ s.c_id[j]) & kMask) == 0;
-        if (__any_sync(kFull, any)) {
+      const bool repeated = s.ctrl[4] != 0;
+      if (repeated) {  // rare: drop repeated ids (warp 0), then share the count
+        if (warp == 0) {
           int cnt = 0;
           for (int base = 0; base < nsv; base += 32) {
             const int j = base + lane;
@@ -339,32 +375,34 @@ __global__ void __launch_bounds__(W * 32, (W <= 4 ? 8 : 4)) batch_search_kernel(
             int lb = 0;
             bool keep = false;
             if (j < nsv) {
-              id = s.c_id[j];
+              id = sid[j];
               d = s.c_d[j];
               lb = s.s_slb[j];
-              keep = j == 0 || ((s.c_id[j - 1] ^ id) & kMask) != 0;
+              keep = j == 0 || ((sid[j - 1] ^ id) & kMask) != 0;
             }
             const unsigned km = __ballot_sync(kFull, keep);
             __syncwarp();
             if (keep) {
               const int slot = cnt + __popc(km & ((1u << lane) - 1));
-              s.c_id[slot] = id;
+              sid[slot] = id;
               s.c_d[slot] = d;
               s.s_slb[slot] = lb;
             }
             cnt += __popc(km);
             __syncwarp();
           }
-          ns = cnt;
+          if (lane == 0) s.ctrl[5] = cnt;
         }
-        if (lane == 0) s.ctrl[5] = ns;
+        __syncthreads();
+        ns = s.ctrl[5];
       }
-      __syncthreads();
-      ns = s.ctrl[5];
+      // Move old entries and survivors into the other list buffer: old entry i
+      // goes to i + #{survivors inserted at or before i}, survivor r to its
+      // insertion point + r; positions >= L drop.
       const int nsz = min(sz + ns, L);
-      if (ns) {  // B4
+      if (ns) {
         for (int i = tid; i < sz; i += W * 32) {
-          int lo = 0, hi = ns;  // survivors inserted before old entry i
+          int lo = 0, hi = ns;
           while (lo < hi) {
             const int mid = (lo + hi) >> 1;
             if (s.s_slb[mid] <= i) lo = mid + 1; else hi = mid;
@@ -378,10 +416,12 @@ __global__ void __launch_bounds__(W * 32, (W <= 4 ? 8 : 4)) batch_search_kernel(
         for (int r = tid; r < ns; r += W * 32) {
           const int dst = s.s_slb[r] + r;
           if (dst < L) {
-            out_id[dst] = s.c_id[r];
+            out_id[dst] = sid[r];
             out_d[dst] = s.c_d[r];
           }
         }
+        const int first_new = s.s_slb[0];
+        if (first_new < scan_from) scan_from = first_new;
         uint32_t* ti = list_id;
         float* td = list_d;
         list_id = out_id;
@@ -389,39 +429,13 @@ __global__ void __launch_bounds__(W * 32, (W <= 4 ? 8 : 4)) batch_search_kernel(
         out_id = ti;
         out_d = td;
       }
-      const int first_new = ns ? s.s_slb[0] : INT_MAX;
       sz = nsz;
-      __syncthreads();
-      if (warp == 0) {  // B5: next selection, the first W unexpanded entries
-        if (first_new < scan_from) scan_from = first_new;
-        int nnext = 0;
-        for (int base = scan_from; base < sz && nnext < W; base += 32) {
-          const int i = base + lane;
-          unsigned um = __ballot_sync(kFull, i < sz && !(list_id[i] & kExpanded));
-          if (base == scan_from && um == 0) scan_from = min(base + 32, sz);
-          while (um && nnext < W) {
-            const int b = __ffs(um) - 1;
-            um &= um - 1;
-            const uint32_t id = list_id[base + b] & kMask;
-            if (lane == 0) {
-              s.sel_id[nnext] = (int32_t)id;
-              list_id[base + b] |= kExpanded;
-            }
-            // start pulling the record toward L2 before the barrier
-            if (lane == nnext && id < (uint32_t)p.n)
-              prefetch_record(p.ix.pages + ((int64_t)id / p.npp) * kPageSize + ((int64_t)id % p.npp) * p.node_len,
-                              (int)p.node_len);
-            nnext++;
-          }
-          __syncwarp();
-        }
-        if (lane == 0) {
-          s.ctrl[1] = (hops + nnext > kHopCap) ? 0 : nnext;
-          s.ctrl[2] = 0;
-          if (hops + nnext > kHopCap) atomicOr(p.err, kErrHopCap);
-        }
-      }
-      __syncthreads();
+      // Every thread read the survivor count after (1); the next step adds to
+      // it only after (3), so it is reset here. The repeat flag is read by every
+      // thread after (2) and set again only after the next (1).
+      if (tid == 0) s.ctrl[2] = 0;
+      __syncthreads();  // (3) the new list is complete
+      if (tid == 0) s.ctrl[4] = 0;
     }
     // outputs (warp 0 holds the top-k bookkeeping)
     if (warp == 0) {
