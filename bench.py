@@ -425,6 +425,10 @@ def _run_ours(args, rank, world, local):
                "batched_bf16x3": BatchRunner(g, q, k, gb.PREC_BF16X3, args.beam, "batched_bf16x3"),
                "batched_fp32": BatchRunner(g, q, k, gb.PREC_FP32, args.beam, "batched_fp32")}
     forms = [f for f in args.forms.split(",") if f in runners]
+    tuned = None
+    if args.beam == 0 and any(f != "plain" for f in forms):  # autotuner: beam width and visited cache
+        W, hb, secs = g.autotune(q.data_ptr(), q.shape[0], k, args.tune_L, gb.PREC_BF16)
+        tuned = {"beam_width": W, "hash_bits": hb, "at_L": args.tune_L, "seconds": secs}
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     res = {f: measure_form(runners[f], args, gt, world, flush, local) for f in forms}
     ok = [f for f in forms if res[f]["recall"] >= args.recall]
@@ -445,7 +449,9 @@ def _run_ours(args, rank, world, local):
                 f"{'SIFT' if meta['kind'] == 'u8' else 'DEEP'}; index built on the device",
         "config": {"workload": args.workload, "n": meta["n"], "dim": meta["dim"], "vector": meta["kind"],
                    "R": meta["R"], "pq_chunks": meta["M"], "nav_points": meta["nav"], "queries_per_step": nq,
-                   "k": k, "L": r["L"], "form": head, "beam_width": args.beam if head != "plain" else 1,
+                   "k": k, "L": r["L"], "form": head,
+                   "beam_width": (tuned["beam_width"] if tuned else args.beam) if head != "plain" else 1,
+                   "autotune": tuned,
                    "l2": "flushed (256 MB write) before every step", "parallelism": f"replicas x{world}"},
         "recall": r["recall"], "recall_target": args.recall,
         "hops_per_query": r["hops_per_query"],
@@ -580,7 +586,8 @@ def main():
     ap.add_argument("--no-ref-gpu", action="store_true")
     ap.add_argument("--forms", default="plain,batched_bf16,batched_bf16x3,batched_fp32")
     ap.add_argument("--headline", default="batched_bf16")
-    ap.add_argument("--beam", type=int, default=4)
+    ap.add_argument("--beam", type=int, default=0, help="0 = autotune (gann_autotune)")
+    ap.add_argument("--tune-L", type=int, default=384)
     args = ap.parse_args()
     rank, world, local = dist_env()
     if args.impl == "reference":

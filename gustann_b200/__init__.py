@@ -24,7 +24,7 @@ import numpy as np
 _LIB_PATH = Path(__file__).resolve().parent / "libgann.so"
 _lib = None
 
-GANN_OK, GANN_EINVAL, GANN_EIO, GANN_EFORMAT, GANN_ECUDA, GANN_ENOMEM, GANN_EKERNEL, GANN_ERANGE = range(8)
+GANN_OK, GANN_EINVAL, GANN_EIO, GANN_EFORMAT, GANN_ECUDA, GANN_ENOMEM, GANN_EKERNEL, GANN_ERANGE, GANN_EBUSY = range(9)
 PREC_FP32, PREC_BF16, PREC_BF16X3, PREC_BF16_CC = 0, 1, 2, 3
 
 
@@ -64,6 +64,23 @@ class BatchOpts(ctypes.Structure):
                 ("reserved", ctypes.c_int32 * 5)]
 
 
+class ServerOpts(ctypes.Structure):
+    """gann_server_opts_t (include/gann.h)."""
+
+    _fields_ = [("max_batch", ctypes.c_int32), ("streams", ctypes.c_int32), ("topk_max", ctypes.c_int32),
+                ("ef_max", ctypes.c_int32), ("precision", ctypes.c_int32), ("beam_width", ctypes.c_int32),
+                ("hash_bits", ctypes.c_int32), ("max_wait_us", ctypes.c_int32), ("min_batch", ctypes.c_int32),
+                ("reserved", ctypes.c_int32 * 7)]
+
+
+class LoadStats(ctypes.Structure):
+    """gann_load_stats_t (include/gann.h)."""
+
+    _fields_ = [("offered_qps", ctypes.c_double), ("achieved_qps", ctypes.c_double), ("submitted", ctypes.c_int64),
+                ("rejected", ctypes.c_int64), ("completed", ctypes.c_int64), ("p50_ms", ctypes.c_double),
+                ("p99_ms", ctypes.c_double), ("p999_ms", ctypes.c_double), ("mean_ms", ctypes.c_double)]
+
+
 class GannInfo(ctypes.Structure):
     _fields_ = [
         ("num_points", ctypes.c_int64), ("dim", ctypes.c_int64), ("max_degree", ctypes.c_int64),
@@ -87,6 +104,13 @@ _SIGNATURES = {
     "gann_search_batch_device": (_I, [_P, _P, _I, _P, _P, _I, _I, _P, _P, _P, _P, _P, _P, _P]),
     "gann_search_batch_noalloc": (_I, [_P, _P, _I, _I, _I, _P, _P, _P, _P, _P]),
     "gann_pq_tables": (_I, [_P, _P, _I, _I, _P]),
+    "gann_autotune": (_I, [_P, _P, _I, _I, _I, _I, _P, ctypes.POINTER(ctypes.c_double)]),
+    "gann_server_start": (_I, [_P, ctypes.POINTER(ServerOpts), ctypes.POINTER(_P)]),
+    "gann_server_submit": (_I, [_P, _P, _I, _I, ctypes.c_uint64]),
+    "gann_server_poll": (_I, [_P, _I, _P, _P, _P, _P, _P, ctypes.POINTER(_I)]),
+    "gann_server_stop": (_I, [_P]),
+    "gann_server_open_loop": (_I, [_P, _P, _I, _P, _P, ctypes.c_double, ctypes.c_double, ctypes.c_uint64,
+                                   ctypes.POINTER(LoadStats)]),
     "gann_check": (_I, [_P, _P]),
     "gann_set_fma": (_I, [_P, _I, _I]),
     "gann_last_error": (ctypes.c_char_p, []),
@@ -253,6 +277,15 @@ class GustANN:
                                               ctypes.byref(o), d_nns, d_dists, d_found, d_hops or None,
                                               d_bytes or None, _stream(stream)))
 
+    def autotune(self, d_q: int, nq: int, topk: int, ef_search: int, precision: int = PREC_BF16):
+        """gann_autotune: returns (beam_width, hash_bits, seconds) of the fastest
+        configuration, which becomes this handle's default."""
+        o = BatchOpts()
+        t = ctypes.c_double(0.0)
+        _check(lib().gann_autotune(self.handle, d_q, nq, topk, ef_search, int(precision), ctypes.byref(o),
+                                   ctypes.byref(t)))
+        return o.beam_width, o.hash_bits, t.value
+
     def pq_tables(self, q: np.ndarray, precision: int) -> np.ndarray:
         """PQ tables (nq x M x 256, FP32 view) as the given precision builds them."""
         q = np.ascontiguousarray(q, dtype=np.float32)
@@ -272,5 +305,65 @@ class GustANN:
     def __del__(self):
         try:
             self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Continuous-batching server over one open index (gann_server_*)."""
+
+    def __init__(self, index: GustANN, max_batch: int = 1024, streams: int = 4, topk_max: int = 100,
+                 ef_max: int = 512, precision: int = PREC_BF16, beam_width: int = 0, hash_bits: int = 0,
+                 max_wait_us: int = 100, min_batch: int = 0):
+        self.index = index
+        self.dim = index.info()["dim"]
+        o = ServerOpts()
+        (o.max_batch, o.streams, o.topk_max, o.ef_max, o.precision, o.beam_width, o.hash_bits, o.max_wait_us,
+         o.min_batch) = (max_batch, streams, topk_max, ef_max, precision, beam_width, hash_bits, max_wait_us,
+                         min_batch)
+        self.topk_max = topk_max
+        self._s = _P()
+        _check(lib().gann_server_start(index.handle, ctypes.byref(o), ctypes.byref(self._s)))
+
+    def submit(self, query: np.ndarray, topk: int, ef_search: int, tag: int) -> bool:
+        """False when the server's request budget is full (GANN_EBUSY)."""
+        q = np.ascontiguousarray(query, dtype=np.float32).reshape(-1)
+        rc = lib().gann_server_submit(self._s, _ptr(q), int(topk), int(ef_search), int(tag))
+        if rc == GANN_EBUSY:
+            return False
+        _check(rc)
+        return True
+
+    def poll(self, max_results: int = 4096):
+        tags = np.zeros(max_results, np.uint64)
+        ids = np.zeros((max_results, self.topk_max), np.int32)
+        dis = np.zeros((max_results, self.topk_max), np.float32)
+        fnd = np.zeros(max_results, np.int32)
+        lat = np.zeros(max_results, np.float64)
+        n = ctypes.c_int(0)
+        _check(lib().gann_server_poll(self._s, max_results, _ptr(tags), _ptr(ids), _ptr(dis), _ptr(fnd), _ptr(lat),
+                                      ctypes.byref(n)))
+        k = n.value
+        return tags[:k], ids[:k], dis[:k], fnd[:k], lat[:k]
+
+    def open_loop(self, queries: np.ndarray, rate_qps: float, seconds: float, topk=None, ef_search=None,
+                  seed: int = 1) -> dict:
+        q = np.ascontiguousarray(queries, dtype=np.float32)
+        ka = None if topk is None else np.ascontiguousarray(topk, dtype=np.int32)
+        la = None if ef_search is None else np.ascontiguousarray(ef_search, dtype=np.int32)
+        st = LoadStats()
+        _check(lib().gann_server_open_loop(self._s, _ptr(q), q.shape[0], None if ka is None else _ptr(ka),
+                                           None if la is None else _ptr(la), float(rate_qps), float(seconds),
+                                           int(seed), ctypes.byref(st)))
+        return {f: getattr(st, f) for f, _ in LoadStats._fields_}
+
+    def stop(self) -> None:
+        if self._s:
+            lib().gann_server_stop(self._s)
+            self._s = None
+
+    def __del__(self):
+        try:
+            self.stop()
         except Exception:
             pass

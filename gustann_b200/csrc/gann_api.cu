@@ -391,16 +391,19 @@ int batch_hash_bits(int ef_max) {
   return b;
 }
 
+// Enqueue one batched search. counter / tables: caller-owned work counter and
+// BF16 table buffer (nq x M x 256) for concurrent launches; null = the handle's.
 int enqueue_batch(gann_t* h, const float* d_q, int nq, const int32_t* d_k, const int32_t* d_l, int k_max,
                   int l_max, const gann_batch_opts_t* opts, int32_t* d_nns, float* d_dists, int32_t* d_found,
-                  int32_t* d_hops, int64_t* d_bytes, cudaStream_t s) {
+                  int32_t* d_hops, int64_t* d_bytes, cudaStream_t s, int* counter = nullptr,
+                  __nv_bfloat16* tables = nullptr) {
   gann_batch_opts_t o{};
   if (opts) o = *opts;
   const int prec = opts ? o.precision : GANN_PREC_BF16;
-  const int W = o.beam_width ? o.beam_width : 4;
+  const int W = o.beam_width ? o.beam_width : (h->tuned_beam ? h->tuned_beam : 4);
   if (!(W == 1 || W == 2 || W == 4 || W == 8)) return set_error(GANN_EINVAL, "beam_width must be 1, 2, 4 or 8");
   if (prec < GANN_PREC_FP32 || prec > GANN_PREC_BF16_CC) return set_error(GANN_EINVAL, "unknown precision");
-  const int hb = o.hash_bits ? o.hash_bits : batch_hash_bits(l_max);
+  const int hb = o.hash_bits ? o.hash_bits : batch_hash_bits(l_max) + h->tuned_hash_delta;
   if (hb < 4 || hb > 16) return set_error(GANN_EINVAL, "hash_bits must be in 4..16");
   const bool bf16 = prec != GANN_PREC_FP32;
   const size_t smem = gann::batch_smem_bytes(h->hx.pq_m, bf16 ? 2 : 4, hb, l_max, (int)h->hx.max_m0, W, k_max,
@@ -434,14 +437,14 @@ int enqueue_batch(gann_t* h, const float* d_q, int nq, const int32_t* d_k, const
   p.found = d_found;
   p.hops = d_hops;
   p.bytes = d_bytes;
-  p.next_query = h->d_counter;
+  p.next_query = counter ? counter : h->d_counter;
   p.err = h->d_err;
   cudaError_t e = cudaSuccess;
   if ((prec == GANN_PREC_BF16 || prec == GANN_PREC_BF16X3) && !h->dx.tc_bpanel_hi)
     return set_error(GANN_ERANGE, "tensor-core tables need PQ chunks of at most 16 dimensions");
   if (prec == GANN_PREC_BF16 || prec == GANN_PREC_BF16X3) {
     const size_t need = (size_t)nq * h->hx.pq_m * gann::kPivots;
-    if (need > h->cap_tables) {
+    if (!tables && need > h->cap_tables) {
       if (h->d_tables) cudaFree(h->d_tables);
       h->d_tables = nullptr;
       h->cap_tables = 0;
@@ -449,12 +452,13 @@ int enqueue_batch(gann_t* h, const float* d_q, int nq, const int32_t* d_k, const
       if (e != cudaSuccess) return set_error(GANN_ENOMEM, "cannot allocate the batch's BF16 tables");
       h->cap_tables = need;
     }
-    e = gann::launch_table_tc(h->dx, (int)h->hx.dim, h->hx.pq_m, d_q, nq, prec == GANN_PREC_BF16X3, h->d_tables, s);
+    __nv_bfloat16* tab = tables ? tables : h->d_tables;
+    e = gann::launch_table_tc(h->dx, (int)h->hx.dim, h->hx.pq_m, d_q, nq, prec == GANN_PREC_BF16X3, tab, s);
     if (e != cudaSuccess) return set_error(GANN_ECUDA, std::string("table build: ") + cudaGetErrorString(e));
-    p.tables = h->d_tables;
+    p.tables = tab;
   }
   if (d_bytes) e = cudaMemsetAsync(d_bytes, 0, sizeof(int64_t) * nq, s);
-  if (e == cudaSuccess) e = cudaMemsetAsync(h->d_counter, 0, sizeof(int), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(p.next_query, 0, sizeof(int), s);
   if (e == cudaSuccess) e = gann::launch_batch(p, h->hx.dtype, bf16, W, h->num_sms, s);
   if (e != cudaSuccess) return set_error(GANN_ECUDA, std::string("batch search launch: ") + cudaGetErrorString(e));
   return GANN_OK;
@@ -592,6 +596,67 @@ int gann_pq_tables(gann_t* h, const float* queries, int nq, int precision, float
   return GANN_OK;
 }
 
+int gann_autotune(gann_t* h, const float* d_queries, int nq, int topk, int ef_search, int precision,
+                  gann_batch_opts_t* best, double* best_seconds) {
+  int rc = check_batch_args(h, nq, topk, ef_search);
+  if (rc) return rc;
+  if (nq < 1 || !d_queries) return set_error(GANN_EINVAL, "autotune needs queries");
+  int32_t *d_nns = nullptr, *d_found = nullptr;
+  float* d_dists = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaError_t e = cudaMalloc(&d_nns, sizeof(int32_t) * (size_t)nq * topk);
+  if (e == cudaSuccess) e = cudaMalloc(&d_dists, sizeof(float) * (size_t)nq * topk);
+  if (e == cudaSuccess) e = cudaMalloc(&d_found, sizeof(int32_t) * (size_t)nq);
+  if (e == cudaSuccess) e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
+  double best_t = 1e30;
+  gann_batch_opts_t best_o{};
+  int best_delta = 0;
+  if (e == cudaSuccess) {
+    std::lock_guard<std::mutex> lk(h->mu);
+    cudaStream_t s = h->stream;
+    const int base_bits = batch_hash_bits(ef_search);
+    for (int W : {2, 4, 8}) {
+      for (int delta : {-1, 0, 1}) {
+        gann_batch_opts_t o{};
+        o.precision = precision;
+        o.beam_width = W;
+        o.hash_bits = base_bits + delta;
+        double t = 1e30;
+        bool ok = true;
+        for (int rep = 0; rep < 3 && ok; rep++) {
+          cudaEventRecord(e0, s);
+          ok = enqueue_batch(h, d_queries, nq, nullptr, nullptr, topk, ef_search, &o, d_nns, d_dists, d_found,
+                             nullptr, nullptr, s) == GANN_OK;
+          cudaEventRecord(e1, s);
+          float ms = 0.0f;
+          if (ok) ok = cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess;
+          if (ok && rep > 0 && ms * 1e-3 < t) t = ms * 1e-3;  // first run warms caches
+        }
+        if (ok && t < best_t) {
+          best_t = t;
+          best_o = o;
+          best_delta = delta;
+        }
+      }
+    }
+    if (best_t < 1e30) {
+      h->tuned_beam = best_o.beam_width;
+      h->tuned_hash_delta = best_delta;
+    }
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaFree(d_nns);
+  cudaFree(d_dists);
+  cudaFree(d_found);
+  if (e != cudaSuccess) return set_error(GANN_ECUDA, std::string("gann_autotune: ") + cudaGetErrorString(e));
+  if (best_t >= 1e30) return set_error(GANN_ERANGE, "no configuration could run these sizes");
+  if (best) *best = best_o;
+  if (best_seconds) *best_seconds = best_t;
+  return GANN_OK;
+}
+
 /* Synchronise `stream` (NULL = the handle's stream) and report any error word
  * left by kernels launched with gann_search_device; clears it. */
 int gann_check(gann_t* h, void* stream) {
@@ -622,3 +687,13 @@ int gann_set_fma(gann_t* h, int fma_table, int fma_exact) {
 }
 
 }  // extern "C"
+
+// Batched launch with caller-owned counter and tables (the server's batch slots).
+int gann_internal_enqueue_batch(gann_t* h, const float* d_q, int nq, const int32_t* d_k, const int32_t* d_l,
+                                int k_max, int l_max, const gann_batch_opts_t* opts, int32_t* d_nns,
+                                float* d_dists, int32_t* d_found, cudaStream_t s, int* counter,
+                                __nv_bfloat16* tables) {
+  return enqueue_batch(h, d_q, nq, d_k, d_l, k_max, l_max, opts, d_nns, d_dists, d_found, nullptr, nullptr, s,
+                       counter, tables);
+}
+

@@ -163,4 +163,6 @@ struct gann_index {
   __nv_bfloat16* d_tables = nullptr; // BF16 tables of one batch (scratch)
   size_t cap_tables = 0;
   int fma_table = 1, fma_exact = 1;
+  int tuned_beam = 0;       // batched-form defaults chosen by gann_autotune (0 = built-in)
+  int tuned_hash_delta = 0; // added to the L-sized visited-cache bits
 };

@@ -1,0 +1,397 @@
+// Continuous-batching search server over the batched form.
+//
+// The reference answers one fixed batch per call (PureMemExecutor::search,
+// src/pure_mem.cu:71-199). Here requests arrive one by one; a dispatcher thread
+// packs the ones that have arrived into a batch whenever a batch slot is free
+// and launches it on that slot's stream, so requests that arrive while others
+// run on the GPU start as soon as a slot frees up, and up to `streams` batches
+// overlap on the device. Each slot owns its device buffers (queries, per-query
+// k and L, results, work counter, BF16 tables), allocated at start; admission
+// is by that budget: a submit is refused (GANN_EBUSY) while every request slot
+// of the server is taken. Per-query state (candidate list, visited cache,
+// table) lives on the device for the life of its batch. A request's result
+// depends only on the query, its k and L, and the server's options, not on
+// the other requests in its batch.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cstring>
+#include <mutex>
+#include <random>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "gann_internal.h"
+
+int gann_internal_set_error(int code, const char* msg);
+int gann_internal_enqueue_batch(gann_t* h, const float* d_q, int nq, const int32_t* d_k, const int32_t* d_l,
+                                int k_max, int l_max, const gann_batch_opts_t* opts, int32_t* d_nns,
+                                float* d_dists, int32_t* d_found, cudaStream_t s, int* counter,
+                                __nv_bfloat16* tables);
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+double now_s() { return std::chrono::duration<double>(Clock::now().time_since_epoch()).count(); }
+
+struct Slot {
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done = nullptr;
+  float* h_q = nullptr;
+  int32_t *h_k = nullptr, *h_l = nullptr, *h_nns = nullptr, *h_f = nullptr;
+  float* h_d = nullptr;
+  float* d_q = nullptr;
+  int32_t *d_k = nullptr, *d_l = nullptr, *d_nns = nullptr, *d_f = nullptr;
+  float* d_d = nullptr;
+  int* d_counter = nullptr;
+  __nv_bfloat16* d_tab = nullptr;
+  std::vector<uint64_t> tags;
+  std::vector<double> t_submit;
+  int count = 0;
+  bool busy = false;
+};
+
+}  // namespace
+
+struct gann_server {
+  gann_t* h = nullptr;
+  gann_server_opts_t o{};
+  int dim = 0, M = 0;
+  std::vector<Slot> slots;
+  // request ring (host): queries, k, L, tag, submit time
+  int cap = 0, head = 0, tail = 0, size = 0;
+  std::vector<float> rq;
+  std::vector<int32_t> rk, rl;
+  std::vector<uint64_t> rtag;
+  std::vector<double> rt;
+  int in_flight = 0;  // requests inside busy slots
+  // completions (ring of the same capacity; counted against the budget until polled)
+  int dhead = 0, dsize = 0;
+  std::vector<uint64_t> dtag;
+  std::vector<int32_t> dfound, dids;
+  std::vector<float> ddist;
+  std::vector<double> dlat;
+  std::mutex mu;
+  std::thread th;
+  std::atomic<bool> stop{false};
+  std::atomic<int> error{0};
+  std::string error_msg;
+};
+
+namespace {
+
+void free_slot(Slot& s) {
+  for (void* p : {(void*)s.h_q, (void*)s.h_k, (void*)s.h_l, (void*)s.h_nns, (void*)s.h_f, (void*)s.h_d})
+    if (p) cudaFreeHost(p);
+  for (void* p : {(void*)s.d_q, (void*)s.d_k, (void*)s.d_l, (void*)s.d_nns, (void*)s.d_f, (void*)s.d_d,
+                  (void*)s.d_counter, (void*)s.d_tab})
+    if (p) cudaFree(p);
+  if (s.done) cudaEventDestroy(s.done);
+  if (s.stream) cudaStreamDestroy(s.stream);
+  s = Slot{};
+}
+
+cudaError_t alloc_slot(Slot& s, int B, int dim, int kmax, int M, bool tables) {
+  cudaError_t e = cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaMallocHost(&s.h_q, sizeof(float) * (size_t)B * dim);
+  if (e == cudaSuccess) e = cudaMallocHost(&s.h_k, sizeof(int32_t) * B);
+  if (e == cudaSuccess) e = cudaMallocHost(&s.h_l, sizeof(int32_t) * B);
+  if (e == cudaSuccess) e = cudaMallocHost(&s.h_nns, sizeof(int32_t) * (size_t)B * kmax);
+  if (e == cudaSuccess) e = cudaMallocHost(&s.h_d, sizeof(float) * (size_t)B * kmax);
+  if (e == cudaSuccess) e = cudaMallocHost(&s.h_f, sizeof(int32_t) * B);
+  if (e == cudaSuccess) e = cudaMalloc(&s.d_q, sizeof(float) * (size_t)B * dim);
+  if (e == cudaSuccess) e = cudaMalloc(&s.d_k, sizeof(int32_t) * B);
+  if (e == cudaSuccess) e = cudaMalloc(&s.d_l, sizeof(int32_t) * B);
+  if (e == cudaSuccess) e = cudaMalloc(&s.d_nns, sizeof(int32_t) * (size_t)B * kmax);
+  if (e == cudaSuccess) e = cudaMalloc(&s.d_d, sizeof(float) * (size_t)B * kmax);
+  if (e == cudaSuccess) e = cudaMalloc(&s.d_f, sizeof(int32_t) * B);
+  if (e == cudaSuccess) e = cudaMalloc(&s.d_counter, sizeof(int) * 4);
+  if (e == cudaSuccess && tables) e = cudaMalloc(&s.d_tab, sizeof(__nv_bfloat16) * (size_t)B * M * gann::kPivots);
+  s.tags.resize(B);
+  s.t_submit.resize(B);
+  return e;
+}
+
+// Collect finished batches into the completion list. Caller holds mu.
+void harvest(gann_server* sv) {
+  const int kmax = sv->o.topk_max;
+  for (Slot& s : sv->slots) {
+    if (!s.busy) continue;
+    cudaError_t q = cudaEventQuery(s.done);
+    if (q == cudaErrorNotReady) continue;
+    const double t = now_s();
+    if (q != cudaSuccess && !sv->error) {
+      sv->error = GANN_ECUDA;
+      sv->error_msg = std::string("server batch: ") + cudaGetErrorString(q);
+    }
+    for (int i = 0; i < s.count; i++) {
+      const int r = (sv->dhead + sv->dsize) % sv->cap;
+      sv->dtag[r] = s.tags[i];
+      sv->dfound[r] = s.h_f[i];
+      sv->dlat[r] = t - s.t_submit[i];
+      std::memcpy(&sv->dids[(size_t)r * kmax], s.h_nns + (size_t)i * kmax, sizeof(int32_t) * kmax);
+      std::memcpy(&sv->ddist[(size_t)r * kmax], s.h_d + (size_t)i * kmax, sizeof(float) * kmax);
+      sv->dsize++;
+    }
+    sv->in_flight -= s.count;
+    s.busy = false;
+    s.count = 0;
+  }
+}
+
+// Launch the waiting requests on a free slot, if the batching rule allows.
+// Caller holds mu.
+void launch(gann_server* sv) {
+  if (sv->size == 0) return;
+  const int B = sv->o.max_batch;
+  const bool old_enough = now_s() - sv->rt[sv->head] >= sv->o.max_wait_us * 1e-6;
+  if (sv->size < std::min(B, std::max(1, sv->o.min_batch)) && !old_enough) return;
+  Slot* s = nullptr;
+  for (Slot& x : sv->slots)
+    if (!x.busy) {
+      s = &x;
+      break;
+    }
+  if (!s) return;
+  const int n = std::min(B, sv->size), dim = sv->dim;
+  for (int i = 0; i < n; i++) {
+    const int r = sv->head;
+    std::memcpy(s->h_q + (size_t)i * dim, sv->rq.data() + (size_t)r * dim, sizeof(float) * dim);
+    s->h_k[i] = sv->rk[r];
+    s->h_l[i] = sv->rl[r];
+    s->tags[i] = sv->rtag[r];
+    s->t_submit[i] = sv->rt[r];
+    sv->head = (sv->head + 1) % sv->cap;
+    sv->size--;
+  }
+  s->count = n;
+  s->busy = true;
+  sv->in_flight += n;
+  const int kmax = sv->o.topk_max;
+  cudaStream_t st = s->stream;
+  cudaError_t e = cudaMemcpyAsync(s->d_q, s->h_q, sizeof(float) * (size_t)n * dim, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(s->d_k, s->h_k, sizeof(int32_t) * n, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(s->d_l, s->h_l, sizeof(int32_t) * n, cudaMemcpyHostToDevice, st);
+  int rc = GANN_OK;
+  if (e == cudaSuccess) {
+    gann_batch_opts_t bo{};
+    bo.precision = sv->o.precision;
+    bo.beam_width = sv->o.beam_width;
+    bo.hash_bits = sv->o.hash_bits;
+    std::lock_guard<std::mutex> lk(sv->h->mu);
+    rc = gann_internal_enqueue_batch(sv->h, s->d_q, n, s->d_k, s->d_l, kmax, sv->o.ef_max, &bo, s->d_nns, s->d_d,
+                                     s->d_f, st, s->d_counter, s->d_tab);
+  }
+  if (e == cudaSuccess && rc == GANN_OK)
+    e = cudaMemcpyAsync(s->h_nns, s->d_nns, sizeof(int32_t) * (size_t)n * kmax, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess && rc == GANN_OK)
+    e = cudaMemcpyAsync(s->h_d, s->d_d, sizeof(float) * (size_t)n * kmax, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess && rc == GANN_OK)
+    e = cudaMemcpyAsync(s->h_f, s->d_f, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaEventRecord(s->done, st);
+  if ((e != cudaSuccess || rc != GANN_OK) && !sv->error) {
+    sv->error = rc != GANN_OK ? rc : GANN_ECUDA;
+    sv->error_msg = rc != GANN_OK ? "server launch failed" : std::string("server: ") + cudaGetErrorString(e);
+  }
+}
+
+void dispatcher(gann_server* sv) {
+  int prev = -1;
+  cudaGetDevice(&prev);
+  cudaSetDevice(sv->h->device);
+  while (!sv->stop.load(std::memory_order_relaxed)) {
+    bool idle;
+    {
+      std::lock_guard<std::mutex> lk(sv->mu);
+      harvest(sv);
+      launch(sv);
+      idle = sv->size == 0 && sv->in_flight == 0;
+    }
+    if (idle)
+      std::this_thread::sleep_for(std::chrono::microseconds(20));
+    else
+      std::this_thread::yield();
+  }
+  std::lock_guard<std::mutex> lk(sv->mu);
+  for (Slot& s : sv->slots)
+    if (s.busy) cudaEventSynchronize(s.done);
+  harvest(sv);
+}
+
+}  // namespace
+
+extern "C" {
+
+int gann_server_start(gann_t* h, const gann_server_opts_t* opts, gann_server_t** out) {
+  if (!h || !out) return gann_internal_set_error(GANN_EINVAL, "null argument");
+  *out = nullptr;
+  gann_server_opts_t o{};
+  if (opts) o = *opts;
+  if (!o.max_batch) o.max_batch = 1024;
+  if (!o.streams) o.streams = 4;
+  if (!o.topk_max) o.topk_max = 100;
+  if (!o.ef_max) o.ef_max = 512;
+  if (!o.max_wait_us) o.max_wait_us = 100;
+  if (!opts) o.precision = GANN_PREC_BF16;
+  if (o.max_batch < 1 || o.streams < 1 || o.streams > 64 || o.topk_max < 1 || o.ef_max < 1 || o.topk_max > 4096 ||
+      o.ef_max > 4096 || o.max_wait_us < 0)
+    return gann_internal_set_error(GANN_EINVAL, "bad server options");
+  const bool tables = o.precision == GANN_PREC_BF16 || o.precision == GANN_PREC_BF16X3;
+  auto* sv = new gann_server();
+  sv->h = h;
+  sv->o = o;
+  sv->dim = (int)h->hx.dim;
+  sv->M = h->hx.pq_m;
+  sv->cap = o.max_batch * (o.streams + 1);
+  sv->rq.resize((size_t)sv->cap * sv->dim);
+  sv->rk.resize(sv->cap);
+  sv->rl.resize(sv->cap);
+  sv->rtag.resize(sv->cap);
+  sv->rt.resize(sv->cap);
+  sv->dtag.resize(sv->cap);
+  sv->dfound.resize(sv->cap);
+  sv->dlat.resize(sv->cap);
+  sv->dids.resize((size_t)sv->cap * o.topk_max);
+  sv->ddist.resize((size_t)sv->cap * o.topk_max);
+  sv->slots.resize(o.streams);
+  int prev = -1;
+  cudaGetDevice(&prev);
+  cudaSetDevice(h->device);
+  cudaError_t e = cudaSuccess;
+  for (Slot& s : sv->slots) {
+    e = alloc_slot(s, o.max_batch, sv->dim, o.topk_max, sv->M, tables);
+    if (e != cudaSuccess) break;
+  }
+  if (prev >= 0) cudaSetDevice(prev);
+  if (e != cudaSuccess) {
+    for (Slot& s : sv->slots) free_slot(s);
+    delete sv;
+    return gann_internal_set_error(GANN_ENOMEM, (std::string("server buffers: ") + cudaGetErrorString(e)).c_str());
+  }
+  sv->th = std::thread(dispatcher, sv);
+  *out = sv;
+  return GANN_OK;
+}
+
+int gann_server_submit(gann_server_t* sv, const float* query, int topk, int ef_search, uint64_t tag) {
+  if (!sv || !query) return gann_internal_set_error(GANN_EINVAL, "null argument");
+  if (topk < 1 || topk > sv->o.topk_max || ef_search < 1 || ef_search > sv->o.ef_max)
+    return gann_internal_set_error(GANN_EINVAL, "topk / ef_search outside the server's limits");
+  std::lock_guard<std::mutex> lk(sv->mu);
+  if (sv->error) return gann_internal_set_error(sv->error, sv->error_msg.c_str());
+  // admission: waiting + on the GPU + finished but not yet polled, against the budget
+  if (sv->size + sv->in_flight + sv->dsize >= sv->cap) return GANN_EBUSY;
+  const int r = sv->tail;
+  std::memcpy(sv->rq.data() + (size_t)r * sv->dim, query, sizeof(float) * sv->dim);
+  sv->rk[r] = topk;
+  sv->rl[r] = ef_search;
+  sv->rtag[r] = tag;
+  sv->rt[r] = now_s();
+  sv->tail = (sv->tail + 1) % sv->cap;
+  sv->size++;
+  return GANN_OK;
+}
+
+int gann_server_poll(gann_server_t* sv, int max_results, uint64_t* tags, int32_t* nns, float* distances,
+                     int32_t* found_cnt, double* latency, int* n_out) {
+  if (!sv || !n_out) return gann_internal_set_error(GANN_EINVAL, "null argument");
+  *n_out = 0;
+  std::lock_guard<std::mutex> lk(sv->mu);
+  const int n = std::min(max_results, sv->dsize);
+  const int kmax = sv->o.topk_max;
+  for (int i = 0; i < n; i++) {
+    const int r = (sv->dhead + i) % sv->cap;
+    if (tags) tags[i] = sv->dtag[r];
+    if (nns) std::memcpy(nns + (size_t)i * kmax, &sv->dids[(size_t)r * kmax], sizeof(int32_t) * kmax);
+    if (distances) std::memcpy(distances + (size_t)i * kmax, &sv->ddist[(size_t)r * kmax], sizeof(float) * kmax);
+    if (found_cnt) found_cnt[i] = sv->dfound[r];
+    if (latency) latency[i] = sv->dlat[r];
+  }
+  sv->dhead = (sv->dhead + n) % sv->cap;
+  sv->dsize -= n;
+  *n_out = n;
+  if (sv->error) return gann_internal_set_error(sv->error, sv->error_msg.c_str());
+  return GANN_OK;
+}
+
+int gann_server_stop(gann_server_t* sv) {
+  if (!sv) return GANN_OK;
+  sv->stop = true;
+  if (sv->th.joinable()) sv->th.join();
+  int prev = -1;
+  cudaGetDevice(&prev);
+  cudaSetDevice(sv->h->device);
+  for (Slot& s : sv->slots) free_slot(s);
+  if (prev >= 0) cudaSetDevice(prev);
+  delete sv;
+  return GANN_OK;
+}
+
+int gann_server_open_loop(gann_server_t* sv, const float* queries, int nq, const int32_t* topk,
+                          const int32_t* ef_search, double rate_qps, double seconds, uint64_t seed,
+                          gann_load_stats_t* out) {
+  if (!sv || !queries || nq < 1 || rate_qps <= 0 || seconds <= 0 || !out)
+    return gann_internal_set_error(GANN_EINVAL, "bad open-loop arguments");
+  std::mt19937_64 rng(seed);
+  std::exponential_distribution<double> gap(rate_qps);
+  std::vector<double> lat;
+  lat.reserve((size_t)(rate_qps * seconds * 1.1) + 16);
+  const int poll_max = 4096;
+  std::vector<double> lbuf(poll_max);
+  int64_t submitted = 0, rejected = 0;
+  auto drain = [&]() {
+    int n = 0;
+    gann_server_poll(sv, poll_max, nullptr, nullptr, nullptr, nullptr, lbuf.data(), &n);
+    lat.insert(lat.end(), lbuf.begin(), lbuf.begin() + n);
+  };
+  const double t0 = now_s();
+  double next = t0 + gap(rng);
+  int64_t i = 0;
+  while (true) {
+    const double t = now_s();
+    if (t - t0 >= seconds) break;
+    if (t >= next) {
+      const int q = (int)(i % nq);
+      const int rc = gann_server_submit(sv, queries + (size_t)q * sv->dim, topk ? topk[q] : std::min(10, sv->o.topk_max),
+                                        ef_search ? ef_search[q] : sv->o.ef_max, (uint64_t)i);
+      if (rc == GANN_OK)
+        submitted++;
+      else if (rc == GANN_EBUSY)
+        rejected++;
+      else
+        return rc;
+      i++;
+      next += gap(rng);
+    } else if ((i & 63) == 0) {
+      drain();
+    }
+    if ((i & 255) == 0) drain();
+  }
+  const double t_end = now_s();
+  double t_last = t_end;
+  while ((int64_t)lat.size() < submitted && now_s() - t_end < 30.0) {
+    const size_t before = lat.size();
+    drain();
+    if (lat.size() > before) t_last = now_s();
+    std::this_thread::sleep_for(std::chrono::microseconds(20));
+  }
+  std::sort(lat.begin(), lat.end());
+  auto pct = [&](double p) { return lat.empty() ? 0.0 : lat[std::min(lat.size() - 1, (size_t)(p * lat.size()))]; };
+  double mean = 0.0;
+  for (double x : lat) mean += x;
+  out->offered_qps = rate_qps;
+  out->submitted = submitted;
+  out->rejected = rejected;
+  out->completed = (int64_t)lat.size();
+  out->achieved_qps = (double)lat.size() / std::max(seconds, t_last - t0);
+  out->p50_ms = pct(0.50) * 1e3;
+  out->p99_ms = pct(0.99) * 1e3;
+  out->p999_ms = pct(0.999) * 1e3;
+  out->mean_ms = lat.empty() ? 0.0 : mean / lat.size() * 1e3;
+  return GANN_OK;
+}
+
+}  // extern "C"

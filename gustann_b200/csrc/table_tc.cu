@@ -155,6 +155,9 @@ __global__ void __launch_bounds__(kTile, 1) table_tc_kernel(TcParams p) {
   const int q0 = blockIdx.x * kTile;
   const int qi = q0 + tid;
   const int G = kK / p.p;
+  // chunk range of this CTA: whole groups, split over gridDim.y
+  const int gpb = (p.groups + gridDim.y - 1) / gridDim.y;
+  const int c_begin = min(p.M, (int)blockIdx.y * gpb * G), c_end = min(p.M, ((int)blockIdx.y + 1) * gpb * G);
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
@@ -169,7 +172,7 @@ __global__ void __launch_bounds__(kTile, 1) table_tc_kernel(TcParams p) {
   }
   // A operand: residual r = q - mu of this thread's query, split BF16 hi/lo,
   // in each chunk's slot of its group; squared norms per chunk in FP32.
-  for (int c = 0; c < p.M; c++) {
+  for (int c = c_begin; c < c_end; c++) {
     const int b = __ldg(p.chunk_off + c), e = __ldg(p.chunk_off + c + 1);
     const int g = c / G, slot = (c % G) * p.p;
     float nrm = 0.0f;
@@ -187,7 +190,7 @@ __global__ void __launch_bounds__(kTile, 1) table_tc_kernel(TcParams p) {
     rn[(size_t)c * kTile + tid] = nrm;
   }
   // slots of a group not used by any chunk (M not a multiple of G) stay zero
-  for (int c = p.M; c < p.groups * G; c++) {
+  for (int c = max(p.M, c_begin); c < p.groups * G && c_end == p.M && c_begin < p.M; c++) {
     const int g = c / G, slot = (c % G) * p.p;
     for (int t = 0; t < p.p; t++) {
       const int off = umma_kmajor_offset(tid, slot + t);
@@ -203,8 +206,8 @@ __global__ void __launch_bounds__(kTile, 1) table_tc_kernel(TcParams p) {
   const uint32_t b_bytes = kBTileBytes * (p.split3 ? 2u : 1u);
   bool ok = true;
 
-  for (int c = 0; c < p.M && ok; c++) {
-    const uint32_t parity = c & 1;
+  for (int c = c_begin; c < c_end && ok; c++) {
+    const uint32_t parity = (c - c_begin) & 1;
     if (tid == 0) {
       mbar_expect_tx(&bars[0], b_bytes);
       bulk_copy_g2s(b_hi, p.bpanel_hi + (size_t)c * kBTileBytes, kBTileBytes, &bars[0]);
@@ -365,8 +368,10 @@ cudaError_t launch_table_tc(const DeviceIndex& ix, int dim, int M, const float* 
   if (smem > 227 * 1024) return cudaErrorInvalidConfiguration;
   cudaError_t e = cudaFuncSetAttribute(table_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  const int grid = (nq + kTile - 1) / kTile;
-  table_tc_kernel<<<grid, kTile, smem, stream>>>(tp);
+  const int tiles = (nq + kTile - 1) / kTile;
+  int split = (2 * 148 + tiles - 1) / tiles;  // enough CTAs to cover the SMs twice
+  split = std::max(1, std::min(split, ix.tc_groups));
+  table_tc_kernel<<<dim3(tiles, split), kTile, smem, stream>>>(tp);
   return cudaGetLastError();
 }
 

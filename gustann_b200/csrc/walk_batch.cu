@@ -160,10 +160,6 @@ __device__ __forceinline__ float exact_dist(const float* q, const T* v, const fl
   return __shfl_sync(kFull, acc, 0);
 }
 
-__device__ __forceinline__ void prefetch_record(const uint8_t* node, int len) {
-  for (int o = 0; o < len; o += 128) asm volatile("prefetch.global.L2 [%0];" ::"l"(node + o));
-}
-
 // Copy one query's BF16 table (M x 256 x 2 bytes, a multiple of 16) from
 // global memory with 16-byte loads.
 __device__ void copy_table(void* dst, const __nv_bfloat16* src, int bytes, int tid, int nthreads) {

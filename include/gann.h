@@ -31,7 +31,8 @@ enum {
   GANN_ECUDA = 4,    /* a CUDA runtime call failed */
   GANN_ENOMEM = 5,   /* device or host allocation failed */
   GANN_EKERNEL = 6,  /* a kernel reported an error (bad id/degree, wait limit) */
-  GANN_ERANGE = 7    /* a size is beyond what this entry point supports */
+  GANN_ERANGE = 7,   /* a size is beyond what this entry point supports */
+  GANN_EBUSY = 8     /* a server's request budget is full: submit again later */
 };
 
 /* element type of the base vectors; gustann::DataType, src/common.hpp:22-25 */
@@ -143,6 +144,15 @@ int gann_search_batch_device(gann_t* h, const float* d_queries, int nq, const in
                              const gann_batch_opts_t* opts, int32_t* d_nns, float* d_distances,
                              int32_t* d_found_cnt, int32_t* d_hops, int64_t* d_bytes, void* stream);
 
+/* Autotuner of the batched form: times beam widths {2, 4, 8} and visited
+ * caches of {1/2, 1, 2} x the default size on nq device queries at (topk,
+ * ef_search, precision), keeps the fastest, and makes it this handle's default
+ * for gann_search_batch* calls that leave beam_width / hash_bits at 0. Results
+ * do not depend on the cache size; the beam width changes the walk order. The
+ * reference has a fixed launch shape (src/pure_mem.cu:31,137); no counterpart. */
+int gann_autotune(gann_t* h, const float* d_queries, int nq, int topk, int ef_search, int precision,
+                  gann_batch_opts_t* best, double* best_seconds);
+
 /* gann_search_device plus per-query counters (device arrays of nq, each may be
  * NULL): d_hops = nodes expanded, d_bytes = algorithmic gathered bytes (degree
  * word, neighbour ids, vector and the codes of every scored neighbour per hop,
@@ -177,6 +187,55 @@ int gann_search_batch_noalloc(gann_t* h, const float* d_queries, int nq, int top
  * (PQSearchData::init_query, src/impl/pq.cuh:8-59); the BF16 forms widened
  * from their BF16 values. For table-error studies against an FP64 oracle. */
 int gann_pq_tables(gann_t* h, const float* queries, int nq, int precision, float* tables);
+
+/*
+ * Continuous-batching server over the batched form. Requests arrive one at a
+ * time; a dispatcher thread packs the waiting ones into a batch whenever one of
+ * `streams` batch slots is free (or the oldest has waited max_wait_us) and
+ * launches it on that slot's stream, so later arrivals start while earlier
+ * batches run and several batches overlap on the device. Each slot's device
+ * memory is allocated at start; a submit is refused with GANN_EBUSY while
+ * (waiting + running + finished-but-unpolled) requests fill the budget of
+ * max_batch * (streams + 1). A result depends only on its query, topk,
+ * ef_search and the server options, not on the other requests in its batch.
+ * The reference serves one fixed batch per call (src/pure_mem.cu:71-199);
+ * no counterpart.
+ */
+typedef struct gann_server gann_server_t;
+typedef struct {
+  int32_t max_batch;    /* queries per launch; 0 = 1024 */
+  int32_t streams;      /* batch slots (launches in flight); 0 = 4 */
+  int32_t topk_max;     /* largest topk a request may ask; 0 = 100 */
+  int32_t ef_max;       /* largest ef_search a request may ask; 0 = 512 */
+  int32_t precision;    /* GANN_PREC_*; with opts given, as given */
+  int32_t beam_width;   /* 0 = the handle's default */
+  int32_t hash_bits;    /* 0 = sized from ef_max */
+  int32_t max_wait_us;  /* a batch smaller than min_batch waits this long for company; 0 = 100 */
+  int32_t min_batch;    /* 0 = launch as soon as a slot is free */
+  int32_t reserved[7];
+} gann_server_opts_t;
+
+typedef struct {
+  double offered_qps, achieved_qps;
+  int64_t submitted, rejected, completed;
+  double p50_ms, p99_ms, p999_ms, mean_ms;  /* submit -> result available on the host */
+} gann_load_stats_t;
+
+int gann_server_start(gann_t* h, const gann_server_opts_t* opts, gann_server_t** out);
+/* Copy one query (dim floats) in; GANN_EBUSY when the budget is full. */
+int gann_server_submit(gann_server_t* s, const float* query, int topk, int ef_search, uint64_t tag);
+/* Up to max_results finished requests: tags, nns / distances (rows of
+ * topk_max), found counts, latencies in seconds; *n_out = how many. */
+int gann_server_poll(gann_server_t* s, int max_results, uint64_t* tags, int32_t* nns, float* distances,
+                     int32_t* found_cnt, double* latency, int* n_out);
+/* Finish the running batches and release the server. */
+int gann_server_stop(gann_server_t* s);
+/* Open-loop load: submit the nq host queries cyclically at Poisson arrival
+ * times of rate rate_qps for `seconds` (topk / ef_search per query, or NULL
+ * for 10 / ef_max), then drain; reports latency percentiles and throughput. */
+int gann_server_open_loop(gann_server_t* s, const float* queries, int nq, const int32_t* topk,
+                          const int32_t* ef_search, double rate_qps, double seconds, uint64_t seed,
+                          gann_load_stats_t* out);
 
 /* Synchronise `stream` (NULL = the handle's stream) and report, as
  * GANN_EKERNEL, any error word left by kernels enqueued with

@@ -161,3 +161,17 @@ def test_batch_is_deterministic(scale):
             b = g.search_batch(q, 10, L, precision=prec, beam_width=4, hash_bits=hb)
             np.testing.assert_array_equal(a[0], b[0])
             np.testing.assert_array_equal(a[1].view(np.uint32), b[1].view(np.uint32))
+
+
+@pytest.mark.gpu
+def test_autotune_sets_the_defaults(scale):
+    import torch
+
+    g, q, gt = scale
+    dq = torch.from_numpy(q).cuda()
+    W, hb, secs = g.autotune(dq.data_ptr(), len(q), 10, 128, gb.PREC_BF16)
+    assert W in (2, 4, 8) and 4 <= hb <= 16 and secs > 0
+    tuned = g.search_batch(q, 10, 128, precision=gb.PREC_BF16)
+    explicit = g.search_batch(q, 10, 128, precision=gb.PREC_BF16, beam_width=W, hash_bits=hb)
+    np.testing.assert_array_equal(tuned[0], explicit[0])
+    np.testing.assert_array_equal(tuned[1].view(np.uint32), explicit[1].view(np.uint32))
