@@ -23,6 +23,10 @@ def gpu_available() -> bool:
 
 
 def pytest_collection_modifyitems(config, items):
+    # a GPU test that stops making progress ends the run instead of holding the box
+    for item in items:
+        if "gpu" in item.keywords and item.get_closest_marker("timeout") is None:
+            item.add_marker(pytest.mark.timeout(600, method="thread"))
     if gpu_available():
         return
     skip = pytest.mark.skip(reason="no CUDA device")

@@ -43,12 +43,23 @@ def test_server_same_alone_and_in_the_mix(index, precision):
     assert srv.submit(q[probe], int(k[probe]), int(L[probe]), tag=10**6)
     alone = collect(srv, 1)[10**6]
     n = 600
-    sent = 0
+    res = {}
+
+    def drain():
+        tags, ids, dis, fnd, lat = srv.poll()
+        for t, i_, d, f, l_ in zip(tags, ids, dis, fnd, lat):
+            res[int(t)] = (i_.copy(), d.copy(), int(f), float(l_))
+
+    t0 = time.time()
     for i in range(n):  # the probe again, in the middle of a stream of other requests
+        # finished results count against the budget until polled, so poll while waiting
         while not srv.submit(q[i], int(k[i]), int(L[i]), tag=i):
+            drain()
+            assert time.time() - t0 < 60, "server made no progress"
             time.sleep(0.0005)
-        sent += 1
-    res = collect(srv, n)
+    while len(res) < n and time.time() - t0 < 60:
+        drain()
+        time.sleep(0.001)
     srv.stop()
     assert len(res) == n
     mixed = res[probe]
