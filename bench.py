@@ -336,6 +336,32 @@ def e2e_steps(runner, q_host_pinned, L, steps, warmup):
     return nq / float(np.mean(ts)), h2d, d2h
 
 
+def serving_sweep(g, meta, rates, seconds, max_batch, streams):
+    """Open-loop serving on the same index: Poisson arrivals at each offered
+    rate, per-request k drawn from {1, 10, 100} and L log-uniform over [32, 512],
+    through the continuous-batching server (gann_server_open_loop)."""
+    import gustann_b200 as gb
+
+    rng = np.random.default_rng(3)
+    q = meta["queries"]
+    ks = rng.choice(np.array([1, 10, 100], np.int32), len(q)).astype(np.int32)
+    Ls = np.exp(rng.uniform(np.log(32), np.log(512), len(q))).astype(np.int32)
+    srv = gb.Server(g, max_batch=max_batch, streams=streams, topk_max=100, ef_max=512, precision=gb.PREC_BF16)
+    out = []
+    try:
+        srv.open_loop(q, rates[0], 0.2, topk=ks, ef_search=Ls, seed=99)  # warm-up
+        for i, r in enumerate(rates):
+            st = srv.open_loop(q, r, seconds, topk=ks, ef_search=Ls, seed=i + 1)
+            out.append({"offered_qps": st["offered_qps"], "achieved_qps": st["achieved_qps"],
+                        "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "p999_ms": st["p999_ms"],
+                        "mean_ms": st["mean_ms"], "submitted": st["submitted"], "rejected": st["rejected"],
+                        "completed": st["completed"]})
+    finally:
+        srv.stop()
+    return {"k": [1, 10, 100], "L": "log-uniform [32, 512]", "max_batch": max_batch, "streams": streams,
+            "seconds_per_rate": seconds, "precision": "bf16", "points": out}
+
+
 def cpu_baseline(meta, L, k, budget_s=15.0):
     """The oracle (CPU restatement of the reference path) on all host cores, on a
     bounded sample of the same queries."""
@@ -388,10 +414,10 @@ def run_ours(args, rank, world, local):
         _run_ours(args, rank, world, local)
 
 
-def measure_form(runner, args, gt, world, flush, local):
+def measure_form(runner, args, gt, world, flush, local, fixed_L=None):
     import torch
 
-    L, rec = calibrate(runner, gt, args.k, args.recall, args.L or None)
+    L, rec = calibrate(runner, gt, args.k, args.recall, fixed_L or args.L or None)
     runner.run(L, counters=True)
     torch.cuda.synchronize()
     hops = runner.hops.cpu().numpy()
@@ -424,14 +450,25 @@ def _run_ours(args, rank, world, local):
                "batched_bf16": BatchRunner(g, q, k, gb.PREC_BF16, args.beam, "batched_bf16"),
                "batched_bf16x3": BatchRunner(g, q, k, gb.PREC_BF16X3, args.beam, "batched_bf16x3"),
                "batched_fp32": BatchRunner(g, q, k, gb.PREC_FP32, args.beam, "batched_fp32")}
+    gh = None
+    if any(f.startswith("host_") for f in args.forms.split(",")):
+        # records in pinned host memory (use_gpu_mem = false), read over PCIe/C2C
+        gh = gb.GustANN(dtype)
+        gh.init_pure_mem(gb.GustANNConfig(meta["index_file"], meta["pq_prefix"], meta["nav_dir"] or ""),
+                         use_gpu_mem=False)
+        runners["host_plain"] = PlainRunner(gh, q, k)
+        runners["host_batched_bf16"] = BatchRunner(gh, q, k, gb.PREC_BF16, args.beam, "host_batched_bf16")
     forms = [f for f in args.forms.split(",") if f in runners]
     tuned = None
     if args.beam == 0 and any(f != "plain" for f in forms):  # autotuner: beam width and visited cache
         W, hb, secs = g.autotune(q.data_ptr(), q.shape[0], k, args.tune_L, gb.PREC_BF16)
         tuned = {"beam_width": W, "hash_bits": hb, "at_L": args.tune_L, "seconds": secs}
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-    res = {f: measure_form(runners[f], args, gt, world, flush, local) for f in forms}
-    ok = [f for f in forms if res[f]["recall"] >= args.recall]
+    res = {}
+    for f in forms:  # a host-paged form runs at the L of its HBM twin (same results, same recall)
+        twin = res.get(f[5:]) if f.startswith("host_") else None
+        res[f] = measure_form(runners[f], args, gt, world, flush, local, twin["L"] if twin else None)
+    ok = [f for f in forms if res[f]["recall"] >= args.recall and not f.startswith("host_")]
     head = args.headline if args.headline in ok else (max(ok, key=lambda f: res[f]["qps"]) if ok else forms[0])
     r, runner = res[head], runners[head]
     nq = runner.nq
@@ -473,10 +510,15 @@ def _run_ours(args, rank, world, local):
     }
     if "plain" in res and head != "plain":
         out["speedup_vs_plain"] = r["qps"] / res["plain"]["qps"]
+    if world == 1 and args.serve_rates:
+        rates = [float(x) for x in args.serve_rates.split(",") if x]
+        out["serving"] = serving_sweep(g, meta, rates, args.serve_seconds, args.serve_batch, args.serve_streams)
     if rank == 0 and world == 1 and not args.no_cpu:
         L_ref = res["plain"]["L"] if "plain" in res else r["L"]
         out["cpu_baseline"], _ = cpu_baseline(meta, L_ref, k, args.cpu_budget)
     g.close()
+    if gh is not None:
+        gh.close()
     barrier(world)
     if world > 1:
         import torch.distributed as dist
@@ -588,6 +630,11 @@ def main():
     ap.add_argument("--headline", default="batched_bf16")
     ap.add_argument("--beam", type=int, default=0, help="0 = autotune (gann_autotune)")
     ap.add_argument("--tune-L", type=int, default=384)
+    ap.add_argument("--serve-rates", default="100000,500000,1000000,1500000,2000000",
+                    help="offered QPS of the open-loop serving sweep ('' = skip)")
+    ap.add_argument("--serve-seconds", type=float, default=1.0)
+    ap.add_argument("--serve-batch", type=int, default=1024)
+    ap.add_argument("--serve-streams", type=int, default=8)
     args = ap.parse_args()
     rank, world, local = dist_env()
     if args.impl == "reference":

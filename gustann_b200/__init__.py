@@ -25,6 +25,7 @@ _LIB_PATH = Path(__file__).resolve().parent / "libgann.so"
 _lib = None
 
 GANN_OK, GANN_EINVAL, GANN_EIO, GANN_EFORMAT, GANN_ECUDA, GANN_ENOMEM, GANN_EKERNEL, GANN_ERANGE, GANN_EBUSY = range(9)
+GANN_OPEN_NO_VALIDATE, GANN_OPEN_HOST_PAGES = 1, 2
 PREC_FP32, PREC_BF16, PREC_BF16X3, PREC_BF16_CC = 0, 1, 2, 3
 
 
@@ -88,6 +89,7 @@ class GannInfo(ctypes.Structure):
         ("num_pages", ctypes.c_int64), ("pq_chunks", ctypes.c_int32), ("dtype", ctypes.c_int32),
         ("has_nav", ctypes.c_int32), ("nav_points", ctypes.c_int32), ("nav_max_degree", ctypes.c_int32),
         ("device", ctypes.c_int32), ("device_bytes", ctypes.c_int64),
+        ("host_pages", ctypes.c_int32), ("reserved0", ctypes.c_int32), ("host_bytes", ctypes.c_int64),
     ]
 
 
@@ -174,16 +176,18 @@ class GustANN:
         self._h = None
 
     def init_pure_mem(self, config: GustANNConfig, use_gpu_mem: bool = True, validate: bool = True) -> None:
-        """GustANN::init_pure_mem (src/ssd_search.cu:108-112). Only the HBM-resident
-        mode (``-G``) is provided; ``use_gpu_mem=False`` (records in host DRAM) is refused."""
-        if not use_gpu_mem:
-            raise GustANNError(GANN_EINVAL, "records in host memory (use_gpu_mem=False) are not provided")
+        """GustANN::init_pure_mem (src/ssd_search.cu:108-112). ``use_gpu_mem=True``
+        (``-G``) makes the records resident in HBM; ``False`` keeps them in pinned
+        host memory that the kernels read over PCIe/C2C (src/pure_mem.cu:51-66),
+        with codes, pivots and the pivot graph in HBM. Results are the same."""
         if self._h is not None:
             self.close()
         h = _P()
         nav = config.nav_graph_prefix.encode() if config.nav_graph_prefix else None
         _check(lib().gann_open(config.index_file.encode(), config.pq_file_prefix.encode(), nav,
-                               int(self.data_type), 0 if validate else 1, ctypes.byref(h)))
+                               int(self.data_type),
+                               (0 if validate else GANN_OPEN_NO_VALIDATE) |
+                               (0 if use_gpu_mem else GANN_OPEN_HOST_PAGES), ctypes.byref(h)))
         self._h = h
 
     @property

@@ -92,6 +92,31 @@ void upload_pages(gann_index* h, const std::string& path, uint8_t* dst, int64_t 
   if (!err.empty()) throw gann::GannError{GANN_EIO, err};
 }
 
+// Records-in-host-memory mode (the reference's use_gpu_mem = false,
+// src/pure_mem.cu:51-66): the page body is read straight into pinned, mapped
+// host memory and the kernels read records through its device alias, so every
+// record fetch crosses PCIe/C2C while codes, pivots and the pivot graph stay in HBM.
+uint8_t* host_pages(gann_index* h, const std::string& path, int64_t bytes) {
+  FILE* f = std::fopen(path.c_str(), "rb");
+  if (!f) throw gann::GannError{GANN_EIO, "cannot open " + path};
+  std::unique_ptr<FILE, int (*)(FILE*)> guard(f, std::fclose);
+  std::fseek(f, gann::kPageSize, SEEK_SET);
+  ck(cudaHostAlloc(reinterpret_cast<void**>(&h->host_pages), (size_t)bytes,
+                   cudaHostAllocPortable | cudaHostAllocMapped),
+     "cudaHostAlloc (index pages)");
+  h->host_bytes = bytes;
+  const size_t chunk = 256u << 20;
+  for (int64_t off = 0; off < bytes;) {
+    size_t n = (size_t)std::min<int64_t>(chunk, bytes - off);
+    if (std::fread(h->host_pages + off, 1, n, f) != n)
+      throw gann::GannError{GANN_EIO, "short read of index pages: " + path};
+    off += (int64_t)n;
+  }
+  void* dptr = nullptr;
+  ck(cudaHostGetDevicePointer(&dptr, h->host_pages, 0), "cudaHostGetDevicePointer");
+  return static_cast<uint8_t*>(dptr);
+}
+
 // Load-time check of every record: degree <= max_m0 and neighbour ids in [0, n).
 __global__ void validate_records(const uint8_t* pages, int64_t n, int64_t npp, int64_t node_len,
                                  int64_t data_len, int max_m, unsigned long long* bad) {
@@ -117,6 +142,9 @@ void free_all(gann_index* h) {
   h->d_nns = nullptr;
   h->d_dists = nullptr;
   h->d_found = nullptr;
+  if (h->host_pages) cudaFreeHost(h->host_pages);
+  h->host_pages = nullptr;
+  h->host_bytes = 0;
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -221,8 +249,13 @@ int gann_open(const char* index_file, const char* pq_prefix, const char* nav_dir
     ck(cudaEventCreate(&h->ev1), "cudaEventCreate");
 
     const gann::HostIndex& hx = h->hx;
-    uint8_t* pages = dev_alloc<uint8_t>(h.get(), (size_t)hx.num_pages * gann::kPageSize);
-    upload_pages(h.get(), index_file, pages, hx.num_pages * (int64_t)gann::kPageSize);
+    uint8_t* pages = nullptr;
+    if (flags & GANN_OPEN_HOST_PAGES) {
+      pages = host_pages(h.get(), index_file, hx.num_pages * (int64_t)gann::kPageSize);
+    } else {
+      pages = dev_alloc<uint8_t>(h.get(), (size_t)hx.num_pages * gann::kPageSize);
+      upload_pages(h.get(), index_file, pages, hx.num_pages * (int64_t)gann::kPageSize);
+    }
     h->dx.pages = pages;
     h->dx.codes = upload(h.get(), codes);
     std::vector<float> pivots_t((size_t)hx.dim * gann::kPivots);  // pq_search.cu:86-91
@@ -314,6 +347,8 @@ int gann_get_info(const gann_t* h, gann_info_t* out) {
   out->nav_max_degree = hx.nav_max_m;
   out->device = h->device;
   out->device_bytes = h->device_bytes;
+  out->host_pages = h->host_pages != nullptr;
+  out->host_bytes = h->host_bytes;
   return GANN_OK;
 }
 

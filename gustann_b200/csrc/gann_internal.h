@@ -149,7 +149,9 @@ struct gann_index {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::vector<void*> allocations;  // device allocations owned by the handle
   int64_t device_bytes = 0;
-  int* d_counter = nullptr;        // work counter scratch (plain kernel)
+  uint8_t* host_pages = nullptr;   // pinned, mapped page body (GANN_OPEN_HOST_PAGES)
+  int64_t host_bytes = 0;
+  int* d_counter = nullptr;       // work counter scratch (plain kernel)
   unsigned int* d_err = nullptr;   // kernel error word
   // per-call device buffers, grown on demand
   float* d_q = nullptr;

@@ -115,61 +115,75 @@ cudaError_t alloc_slot(Slot& s, int B, int dim, int kmax, int M, bool tables) {
   return e;
 }
 
-// Collect finished batches into the completion list. Caller holds mu.
-void harvest(gann_server* sv) {
+// Publish a finished batch into the completion ring. Dispatcher thread only.
+// The ring range [dhead + dsize, + count) is free (the admission budget keeps
+// waiting + in flight + completed <= cap), so it is filled without the lock
+// and made visible to gann_server_poll by one locked update of dsize.
+void complete(gann_server* sv, Slot& s, cudaError_t q) {
   const int kmax = sv->o.topk_max;
-  for (Slot& s : sv->slots) {
-    if (!s.busy) continue;
-    cudaError_t q = cudaEventQuery(s.done);
-    if (q == cudaErrorNotReady) continue;
-    const double t = now_s();
-    if (q != cudaSuccess && !sv->error) {
-      sv->error = GANN_ECUDA;
-      sv->error_msg = std::string("server batch: ") + cudaGetErrorString(q);
-    }
-    for (int i = 0; i < s.count; i++) {
-      const int r = (sv->dhead + sv->dsize) % sv->cap;
-      sv->dtag[r] = s.tags[i];
-      sv->dfound[r] = s.h_f[i];
-      sv->dlat[r] = t - s.t_submit[i];
-      std::memcpy(&sv->dids[(size_t)r * kmax], s.h_nns + (size_t)i * kmax, sizeof(int32_t) * kmax);
-      std::memcpy(&sv->ddist[(size_t)r * kmax], s.h_d + (size_t)i * kmax, sizeof(float) * kmax);
-      sv->dsize++;
-    }
-    sv->in_flight -= s.count;
-    s.busy = false;
-    s.count = 0;
+  const double t = now_s();
+  int base;
+  {
+    std::lock_guard<std::mutex> lk(sv->mu);
+    base = sv->dhead + sv->dsize;
   }
+  for (int i = 0; i < s.count; i++) {
+    const int r = (base + i) % sv->cap;
+    sv->dtag[r] = s.tags[i];
+    sv->dfound[r] = s.h_f[i];
+    sv->dlat[r] = t - s.t_submit[i];
+    std::memcpy(&sv->dids[(size_t)r * kmax], s.h_nns + (size_t)i * kmax, sizeof(int32_t) * kmax);
+    std::memcpy(&sv->ddist[(size_t)r * kmax], s.h_d + (size_t)i * kmax, sizeof(float) * kmax);
+  }
+  std::lock_guard<std::mutex> lk(sv->mu);
+  if (q != cudaSuccess && !sv->error) {
+    sv->error_msg = std::string("server batch: ") + cudaGetErrorString(q);
+    sv->error = GANN_ECUDA;
+  }
+  sv->dsize += s.count;
+  sv->in_flight -= s.count;
+  s.busy = false;
+  s.count = 0;
 }
 
 // Launch the waiting requests on a free slot, if the batching rule allows.
-// Caller holds mu.
-void launch(gann_server* sv) {
-  if (sv->size == 0) return;
-  const int B = sv->o.max_batch;
-  const bool old_enough = now_s() - sv->rt[sv->head] >= sv->o.max_wait_us * 1e-6;
-  if (sv->size < std::min(B, std::max(1, sv->o.min_batch)) && !old_enough) return;
+// Dispatcher thread only. The ring entries [head, head + n) stay counted in
+// `size` while they are copied out without the lock, so no submit can reuse
+// them; head and size move in one locked update afterwards.
+bool launch(gann_server* sv) {
   Slot* s = nullptr;
   for (Slot& x : sv->slots)
     if (!x.busy) {
       s = &x;
       break;
     }
-  if (!s) return;
-  const int n = std::min(B, sv->size), dim = sv->dim;
+  if (!s) return false;
+  const int B = sv->o.max_batch, dim = sv->dim;
+  int n, h0;
+  {
+    std::lock_guard<std::mutex> lk(sv->mu);
+    if (sv->size == 0) return false;
+    const bool old_enough = now_s() - sv->rt[sv->head] >= sv->o.max_wait_us * 1e-6;
+    if (sv->size < std::min(B, std::max(1, sv->o.min_batch)) && !old_enough) return false;
+    n = std::min(B, sv->size);
+    h0 = sv->head;
+  }
   for (int i = 0; i < n; i++) {
-    const int r = sv->head;
+    const int r = (h0 + i) % sv->cap;
     std::memcpy(s->h_q + (size_t)i * dim, sv->rq.data() + (size_t)r * dim, sizeof(float) * dim);
     s->h_k[i] = sv->rk[r];
     s->h_l[i] = sv->rl[r];
     s->tags[i] = sv->rtag[r];
     s->t_submit[i] = sv->rt[r];
-    sv->head = (sv->head + 1) % sv->cap;
-    sv->size--;
+  }
+  {
+    std::lock_guard<std::mutex> lk(sv->mu);
+    sv->head = (h0 + n) % sv->cap;
+    sv->size -= n;
+    sv->in_flight += n;
   }
   s->count = n;
   s->busy = true;
-  sv->in_flight += n;
   const int kmax = sv->o.topk_max;
   cudaStream_t st = s->stream;
   cudaError_t e = cudaMemcpyAsync(s->d_q, s->h_q, sizeof(float) * (size_t)n * dim, cudaMemcpyHostToDevice, st);
@@ -192,22 +206,32 @@ void launch(gann_server* sv) {
   if (e == cudaSuccess && rc == GANN_OK)
     e = cudaMemcpyAsync(s->h_f, s->d_f, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaEventRecord(s->done, st);
-  if ((e != cudaSuccess || rc != GANN_OK) && !sv->error) {
-    sv->error = rc != GANN_OK ? rc : GANN_ECUDA;
-    sv->error_msg = rc != GANN_OK ? "server launch failed" : std::string("server: ") + cudaGetErrorString(e);
+  if (e != cudaSuccess || rc != GANN_OK) {
+    std::lock_guard<std::mutex> lk(sv->mu);
+    if (!sv->error) {
+      sv->error_msg = rc != GANN_OK ? "server launch failed" : std::string("server: ") + cudaGetErrorString(e);
+      sv->error = rc != GANN_OK ? rc : GANN_ECUDA;
+    }
   }
+  return true;
 }
 
 void dispatcher(gann_server* sv) {
-  int prev = -1;
-  cudaGetDevice(&prev);
   cudaSetDevice(sv->h->device);
   while (!sv->stop.load(std::memory_order_relaxed)) {
+    bool work = false;
+    for (Slot& s : sv->slots) {
+      if (!s.busy) continue;
+      const cudaError_t q = cudaEventQuery(s.done);
+      if (q == cudaErrorNotReady) continue;
+      complete(sv, s, q);
+      work = true;
+    }
+    work = launch(sv) || work;
+    if (work) continue;
     bool idle;
     {
       std::lock_guard<std::mutex> lk(sv->mu);
-      harvest(sv);
-      launch(sv);
       idle = sv->size == 0 && sv->in_flight == 0;
     }
     if (idle)
@@ -215,10 +239,24 @@ void dispatcher(gann_server* sv) {
     else
       std::this_thread::yield();
   }
-  std::lock_guard<std::mutex> lk(sv->mu);
   for (Slot& s : sv->slots)
-    if (s.busy) cudaEventSynchronize(s.done);
-  harvest(sv);
+    if (s.busy) complete(sv, s, cudaEventSynchronize(s.done));
+}
+
+// Queue one request that arrived at time t. Caller holds mu.
+int submit_locked(gann_server* sv, const float* query, int topk, int ef_search, uint64_t tag, double t) {
+  if (sv->error) return gann_internal_set_error(sv->error, sv->error_msg.c_str());
+  // admission: waiting + on the GPU + finished but not yet polled, against the budget
+  if (sv->size + sv->in_flight + sv->dsize >= sv->cap) return GANN_EBUSY;
+  const int r = sv->tail;
+  std::memcpy(sv->rq.data() + (size_t)r * sv->dim, query, sizeof(float) * sv->dim);
+  sv->rk[r] = topk;
+  sv->rl[r] = ef_search;
+  sv->rtag[r] = tag;
+  sv->rt[r] = t;
+  sv->tail = (sv->tail + 1) % sv->cap;
+  sv->size++;
+  return GANN_OK;
 }
 
 }  // namespace
@@ -281,18 +319,7 @@ int gann_server_submit(gann_server_t* sv, const float* query, int topk, int ef_s
   if (topk < 1 || topk > sv->o.topk_max || ef_search < 1 || ef_search > sv->o.ef_max)
     return gann_internal_set_error(GANN_EINVAL, "topk / ef_search outside the server's limits");
   std::lock_guard<std::mutex> lk(sv->mu);
-  if (sv->error) return gann_internal_set_error(sv->error, sv->error_msg.c_str());
-  // admission: waiting + on the GPU + finished but not yet polled, against the budget
-  if (sv->size + sv->in_flight + sv->dsize >= sv->cap) return GANN_EBUSY;
-  const int r = sv->tail;
-  std::memcpy(sv->rq.data() + (size_t)r * sv->dim, query, sizeof(float) * sv->dim);
-  sv->rk[r] = topk;
-  sv->rl[r] = ef_search;
-  sv->rtag[r] = tag;
-  sv->rt[r] = now_s();
-  sv->tail = (sv->tail + 1) % sv->cap;
-  sv->size++;
-  return GANN_OK;
+  return submit_locked(sv, query, topk, ef_search, tag, now_s());
 }
 
 int gann_server_poll(gann_server_t* sv, int max_results, uint64_t* tags, int32_t* nns, float* distances,
@@ -347,28 +374,34 @@ int gann_server_open_loop(gann_server_t* sv, const float* queries, int nq, const
     gann_server_poll(sv, poll_max, nullptr, nullptr, nullptr, nullptr, lbuf.data(), &n);
     lat.insert(lat.end(), lbuf.begin(), lbuf.begin() + n);
   };
+  // Arrivals follow a Poisson process fixed in advance; each request's latency
+  // is measured from its scheduled arrival, so a generator that falls behind
+  // shows up as latency, not as a lower offered rate.
   const double t0 = now_s();
-  double next = t0 + gap(rng);
+  double next = t0 + gap(rng), last_drain = t0;
   int64_t i = 0;
   while (true) {
     const double t = now_s();
     if (t - t0 >= seconds) break;
     if (t >= next) {
-      const int q = (int)(i % nq);
-      const int rc = gann_server_submit(sv, queries + (size_t)q * sv->dim, topk ? topk[q] : std::min(10, sv->o.topk_max),
-                                        ef_search ? ef_search[q] : sv->o.ef_max, (uint64_t)i);
-      if (rc == GANN_OK)
-        submitted++;
-      else if (rc == GANN_EBUSY)
-        rejected++;
-      else
-        return rc;
-      i++;
-      next += gap(rng);
-    } else if ((i & 63) == 0) {
-      drain();
+      std::lock_guard<std::mutex> lk(sv->mu);
+      for (int b = 0; b < 256 && next <= t && next - t0 < seconds; b++, next += gap(rng), i++) {
+        const int q = (int)(i % nq);
+        const int rc = submit_locked(sv, queries + (size_t)q * sv->dim,
+                                     topk ? topk[q] : std::min(10, sv->o.topk_max),
+                                     ef_search ? ef_search[q] : sv->o.ef_max, (uint64_t)i, next);
+        if (rc == GANN_OK)
+          submitted++;
+        else if (rc == GANN_EBUSY)
+          rejected++;
+        else
+          return rc;
+      }
     }
-    if ((i & 255) == 0) drain();
+    if (t - last_drain > 50e-6) {
+      drain();
+      last_drain = t;
+    }
   }
   const double t_end = now_s();
   double t_last = t_end;

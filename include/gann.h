@@ -40,7 +40,13 @@ enum { GANN_UINT8 = 0, GANN_FLOAT = 1 };
 
 /* gann_open flags */
 enum {
-  GANN_OPEN_NO_VALIDATE = 1 /* skip the load-time check of degrees and neighbour ids */
+  GANN_OPEN_NO_VALIDATE = 1, /* skip the load-time check of degrees and neighbour ids */
+  /* keep the records (vector + degree + neighbour ids) in pinned, mapped host
+   * memory and read them from the kernels over PCIe/C2C; PQ codes, pivots and
+   * the pivot graph stay in HBM. This is init_pure_mem(config, use_gpu_mem = false)
+   * (src/pure_mem.cu:51-66, kernel search_graph_kernel_dram src/impl/pure_mem.cuh:50-241).
+   * Results are identical to the HBM-resident mode. */
+  GANN_OPEN_HOST_PAGES = 2
 };
 
 /* table precision for gann_search_batch */
@@ -74,12 +80,16 @@ typedef struct {
   int32_t nav_max_degree;  /* NavGraph::max_m src/nav_graph.hpp:14 */
   int32_t device;          /* CUDA device the handle lives on */
   int64_t device_bytes;    /* HBM held by the index */
+  int32_t host_pages;      /* records live in pinned host memory (GANN_OPEN_HOST_PAGES) */
+  int32_t reserved0;
+  int64_t host_bytes;      /* pinned host memory held by the index */
 } gann_info_t;
 
 /*
- * Open an index and make it resident in HBM.
+ * Open an index and make it resident in HBM (with GANN_OPEN_HOST_PAGES: the
+ * records in pinned host memory, the rest in HBM).
  * Replaces gustann::GustANN::GustANN(DataType) + GustANN::init_pure_mem(config,
- * use_gpu_mem = true): src/ssd_search.hpp:70,76, src/ssd_search.cu:55-79,108-112,
+ * use_gpu_mem): src/ssd_search.hpp:70,76, src/ssd_search.cu:55-79,108-112,
  * src/pure_mem.cu:27-69. Files: index_file is DiskANN's `_disk.index`
  * (src/layout.cpp:11-69); `<pq_prefix>_pivots.bin` and `<pq_prefix>_compressed.bin`
  * (src/ssd_search.cu:61-63, src/pq_search.cu:56-121); `<nav_dir>/nav_index`,

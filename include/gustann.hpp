@@ -41,13 +41,15 @@ class GustANN {
   GustANN& operator=(const GustANN&) = delete;
   ~GustANN() { gann_close(h_); }
 
-  // GustANN::init_pure_mem (src/ssd_search.cu:108-112); use_gpu_mem must be true.
+  // GustANN::init_pure_mem (src/ssd_search.cu:108-112): use_gpu_mem = true puts
+  // the records in HBM (-G), false keeps them in pinned host memory read by the
+  // kernels over PCIe/C2C (src/pure_mem.cu:51-66).
   void init_pure_mem(const GustANNConfig& cfg, bool use_gpu_mem) {
-    if (!use_gpu_mem) throw std::runtime_error("gann: records in host memory are not provided; use -G");
     gann_close(h_);
     h_ = nullptr;
     const char* nav = cfg.nav_graph_prefix.empty() ? nullptr : cfg.nav_graph_prefix.c_str();
-    check(gann_open(cfg.index_file.c_str(), cfg.pq_file_prefix.c_str(), nav, data_type_, 0, &h_));
+    check(gann_open(cfg.index_file.c_str(), cfg.pq_file_prefix.c_str(), nav, data_type_,
+                    use_gpu_mem ? 0 : GANN_OPEN_HOST_PAGES, &h_));
   }
 
   // GustANN::search (src/ssd_search.hpp:78-80): host buffers, squared L2.

@@ -3,7 +3,8 @@
 // Used by the tests to show that reference-style host code compiles and links
 // against libgann.so unchanged.
 //
-// usage: shim_driver <uint8|float> <index> <pq_prefix> <nav_dir|-> <queries.bin> <topk> <L> <out.bin>
+// usage: shim_driver <uint8|float> <index> <pq_prefix> <nav_dir|-> <queries.bin> <topk> <L> <out.bin> [gpu|dram]
+// gpu (default) is search_mem's -G (records in HBM); dram keeps the records in host memory.
 // queries.bin: int32 nq, int32 dim, nq*dim float32; out.bin: nns, distances, found_cnt.
 #include <cstdio>
 #include <cstring>
@@ -14,11 +15,13 @@
 #include "gustann.hpp"
 
 int main(int argc, char** argv) {
-  if (argc != 9) {
-    std::fprintf(stderr, "usage: %s <uint8|float> <index> <pq_prefix> <nav_dir|-> <queries.bin> <topk> <L> <out>\n",
+  if (argc != 9 && argc != 10) {
+    std::fprintf(stderr,
+                 "usage: %s <uint8|float> <index> <pq_prefix> <nav_dir|-> <queries.bin> <topk> <L> <out> [gpu|dram]\n",
                  argv[0]);
     return 2;
   }
+  const bool use_gpu_mem = argc == 9 || std::strcmp(argv[9], "dram") != 0;
   gustann::DataType dtype = std::strcmp(argv[1], "uint8") == 0 ? gustann::UINT8 : gustann::FLOAT;
   gustann::GustANNConfig cfg;
   cfg.index_file = argv[2];
@@ -34,7 +37,7 @@ int main(int argc, char** argv) {
   std::fclose(f);
   try {
     gustann::GustANN a(dtype);
-    a.init_pure_mem(cfg, /*use_gpu_mem=*/true);
+    a.init_pure_mem(cfg, use_gpu_mem);
     std::unique_ptr<int[]> nns(new int[(size_t)nq * topk]);
     std::unique_ptr<float[]> dis(new float[(size_t)nq * topk]);
     std::unique_ptr<int[]> found(new int[nq]);

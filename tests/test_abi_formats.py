@@ -101,10 +101,23 @@ def test_open_rejects_mismatched_codes(golden, tmp_path):
     assert rc == gb.GANN_EFORMAT and "code count" in msg
 
 
-def test_host_memory_mode_is_refused():
+def test_host_memory_mode_reports_file_errors():
+    """use_gpu_mem=False reads the same files; a missing one is GANN_EIO before any device work."""
     g = gb.GustANN(gb.DataType.UINT8)
-    with pytest.raises(gb.GustANNError):
-        g.init_pure_mem(gb.GustANNConfig("a", "b", ""), use_gpu_mem=False)
+    with pytest.raises(gb.GustANNError) as e:
+        g.init_pure_mem(gb.GustANNConfig("/nonexistent/index", "/nonexistent/pq", ""), use_gpu_mem=False)
+    assert e.value.code == gb.GANN_EIO
+
+
+def test_info_struct_matches_header():
+    """gann_info_t's layout in the ctypes mirror: field order and the trailing host fields."""
+    import re as _re
+
+    text = (ROOT / "include" / "gann.h").read_text()
+    body = _re.search(r"typedef struct \{([^}]*)\} gann_info_t;", text).group(1)
+    names = _re.findall(r"int(?:32|64)_t\s+(\w+);", body)
+    assert names == [f for f, _ in gb.GannInfo._fields_]
+    assert ctypes.sizeof(gb.GannInfo) == 8 * 7 + 4 * 6 + 8 + 4 * 2 + 8
 
 
 def test_sample_pivots_properties():

@@ -177,3 +177,46 @@ def test_corrupt_record_is_reported_not_read(golden, tmp_path):
     # the handle stays usable after the reported error
     with pytest.raises(gb.GustANNError):
         g.query(meta["queries"][:4], 10, 16)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", NAMES)
+def test_host_pages_match_oracle_fixture(golden, name):
+    """use_gpu_mem=False (records in pinned host memory, src/pure_mem.cu:51-66):
+    the same ids, distances and counts as the oracle."""
+    meta = golden[name]
+    exp = np.load(GOLDEN / name / "oracle.npz")
+    g = gb.GustANN(gb.DataType(meta["dtype"]))
+    g.init_pure_mem(gb.GustANNConfig(meta["index_file"], meta["pq_prefix"], meta["nav_dir"] or ""),
+                    use_gpu_mem=False)
+    inf = g.info()
+    assert inf["host_pages"] == 1 and inf["host_bytes"] == inf["num_pages"] * 4096
+    for k, L in meta["cases"]:
+        ids, dis, fnd, _ = g.query(meta["queries"], k, L)
+        assert_same(ids, dis, fnd, exp[f"ids_k{k}_L{L}"], exp[f"dists_k{k}_L{L}"], exp[f"found_k{k}_L{L}"],
+                    f"host pages {name} k={k} L={L}")
+    g.close()
+
+
+@pytest.mark.gpu
+def test_host_pages_match_hbm_at_scale(scale_index):
+    """Both record placements give identical plain and batched results on the
+    200k index; the batched form is deterministic, so its ids match exactly too."""
+    f, q, gt = scale_index
+    cfg = gb.GustANNConfig(f.index_file, f.pq_prefix, f.nav_dir)
+    hbm = gb.GustANN(gb.DataType.UINT8)
+    hbm.init_pure_mem(cfg)
+    host = gb.GustANN(gb.DataType.UINT8)
+    host.init_pure_mem(cfg, use_gpu_mem=False)
+    hi = host.info()
+    assert hi["device_bytes"] + hi["host_bytes"] == hbm.info()["device_bytes"]
+    for k, L in ((10, 64), (100, 128)):
+        a = hbm.query(q, k, L)
+        b = host.query(q, k, L)
+        assert_same(b[0], b[1], b[2], a[0], a[1], a[2], f"host vs hbm plain k={k} L={L}")
+    for prec in (gb.PREC_BF16, gb.PREC_FP32):
+        a = hbm.search_batch(q, 10, 128, precision=prec)
+        b = host.search_batch(q, 10, 128, precision=prec)
+        assert_same(b[0], b[1], b[2], a[0], a[1], a[2], f"host vs hbm batched precision={prec}")
+    hbm.close()
+    host.close()

@@ -34,7 +34,8 @@ def test_shim_reports_open_errors(tmp_path):
 
 
 @pytest.mark.gpu
-def test_shim_driver_matches_oracle(golden, tmp_path, oracle_mod):
+@pytest.mark.parametrize("mem", ["gpu", "dram"])
+def test_shim_driver_matches_oracle(golden, tmp_path, oracle_mod, mem):
     exe = build_driver(tmp_path)
     meta = golden["u8_nav"]
     q = meta["queries"]
@@ -42,7 +43,7 @@ def test_shim_driver_matches_oracle(golden, tmp_path, oracle_mod):
     qf.write_bytes(struct.pack("<ii", *q.shape) + q.tobytes())
     out = tmp_path / "out.bin"
     r = subprocess.run([str(exe), "uint8", meta["index_file"], meta["pq_prefix"], meta["nav_dir"], str(qf), "10", "40",
-                        str(out)], capture_output=True, text=True)
+                        str(out), mem], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
     raw = out.read_bytes()
     nq = q.shape[0]
