@@ -439,6 +439,8 @@ def _run_ours(args, rank, world, local):
 
     cache = Path(args.cache)
     meta = prepare(args.workload, args.nq, cache, local)
+    if args.batch:  # a smaller step over the first queries of the same set
+        meta["queries"], meta["gt"] = meta["queries"][:args.batch], meta["gt"][:args.batch]
     barrier(world)
     dtype = gb.DataType.UINT8 if meta["kind"] == "u8" else gb.DataType.FLOAT
     g = gb.GustANN(dtype)
@@ -630,6 +632,7 @@ def main():
     ap.add_argument("--headline", default="batched_bf16")
     ap.add_argument("--beam", type=int, default=0, help="0 = autotune (gann_autotune)")
     ap.add_argument("--tune-L", type=int, default=384)
+    ap.add_argument("--batch", type=int, default=0, help="queries per step (default: all --nq)")
     ap.add_argument("--serve-rates", default="100000,500000,1000000,1500000,2000000",
                     help="offered QPS of the open-loop serving sweep ('' = skip)")
     ap.add_argument("--serve-seconds", type=float, default=1.0)

@@ -466,6 +466,7 @@ int enqueue_batch(gann_t* h, const float* d_q, int nq, const int32_t* d_k, const
   p.L_max = l_max;
   p.k_max = k_max;
   p.hash_bits = hb;
+  p.npp_div = gann::FastDiv((uint32_t)h->hx.npp);
   p.fma = h->fma_exact;
   p.nns = d_nns;
   p.dists = d_dists;

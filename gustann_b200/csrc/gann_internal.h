@@ -27,6 +27,37 @@ enum : uint32_t {
   kErrWaitLimit = 16u,  // a bounded spin-wait gave up
 };
 
+// Quotient by a divisor d >= 1 fixed at load time, for numerators in [0, 2^31):
+// q = umulhi(n, m) >> s with p = 31 + ceil(log2 d), m = ceil(2^p / d), s = p - 32
+// (Granlund and Montgomery, "Division by invariant integers using
+// multiplication", PLDI 1994). m < 2^32 because d > 2^(ceil(log2 d) - 1), and
+// the rounding error n * (m d - 2^p) / (d 2^p) < 2^-ceil(log2 d) <= 1/d keeps
+// floor(n m / 2^p) = floor(n / d). Record ids are below 2^31.
+struct FastDiv {
+  uint32_t d = 1, m = 0, s = 0;
+  FastDiv() = default;
+  explicit FastDiv(uint32_t div) : d(div) {
+    if (d > 1) {
+      uint32_t l = 0;
+      while ((1ull << l) < d) l++;
+      const uint32_t p = 31 + l;
+      m = (uint32_t)(((1ull << p) + d - 1) / d);
+      s = p - 32;
+    }
+  }
+#ifdef __CUDACC__
+  __host__ __device__
+#endif
+  inline uint32_t div(uint32_t n) const {
+    if (d == 1) return n;
+#ifdef __CUDA_ARCH__
+    return __umulhi(n, m) >> s;
+#else
+    return (uint32_t)(((uint64_t)n * m) >> 32) >> s;
+#endif
+  }
+};
+
 // Host copy of the index files, parsed and checked (gann_io.cpp).
 struct HostIndex {
   int dtype = 0;  // GANN_UINT8 / GANN_FLOAT
@@ -92,6 +123,7 @@ struct BatchParams {
   const int32_t* k_per_q;         // nq or null (then k_max for all)
   int L_max, k_max;
   int hash_bits;                  // visited cache: 1 << hash_bits slots
+  FastDiv npp_div;                // division by nodes per page
   const __nv_bfloat16* tables;    // nq x M x 256 BF16 tables built for the batch, or null
   int fma;
   int32_t* nns;                   // nq x k_max

@@ -123,6 +123,7 @@ extern "C" int gann_search_batch_noalloc(gann_t* h, const float* d_queries, int 
     p.L_max = ef_search;
     p.k_max = topk;
     p.hash_bits = hb;
+    p.npp_div = gann::FastDiv((uint32_t)h->hx.npp);
     p.tables = tc ? tables : nullptr;
     p.fma = h->fma_exact;
     p.nns = d_nns;

@@ -15,7 +15,8 @@
 //     key, which only decreases. So the cache's contents, which depend on the
 //     order of the warps' atomicExch, change the work done but never the result;
 //   * new candidates are merged into the sorted list of L entries by inserting
-//     the survivors only (entries below the list's last key), as in the plain form;
+//     the survivors only (entries below the list's last key), as in the plain
+//     form, in place: only the entries from the first insertion point on move;
 //   * every expanded node's exact distance goes into the top-k
 //     (src/impl/util.cuh:26-46,116-163).
 // L and k may differ per query.
@@ -30,9 +31,9 @@ struct BatchSmem {
   float* q;
   void* table;
   uint32_t* hash;   // visited cache: one id per slot
-  uint32_t *la_id, *lb_id;
-  float *la_d, *lb_d;
-  uint32_t* c_id;  // [0, W): list positions of the picks; then the sorted survivors (W * max_m)
+  uint32_t* l_id;   // sorted candidate list (L), updated in place
+  float* l_d;
+  uint32_t* c_id;  // sorted survivors (W * max_m)
   float* c_d;      // sorted survivor distances
   uint32_t* s_id;  // survivors of the step, unsorted (W * max_m)
   float* s_d;
@@ -42,20 +43,21 @@ struct BatchSmem {
   float* sel_d;     // W exact distances
   int32_t* topk_id;
   float* topk_d;
-  int* ctrl;        // [0] qid, [2] survivors, [3] entry, [4] repeated id, [5] after dedupe, [6] stop
+  int* ctrl;        // [0] qid, [2] survivors, [3] entry, [4] repeated id, [5] after dedupe, [6] stop,
+                    // [7] first insertion point of the step
   uint32_t* wnew;   // W * max_m: per-warp list of newly seen neighbours
 };
 
 struct BatchPlan {
-  size_t off[19];
+  size_t off[17];
   size_t total;
   __host__ __device__ BatchPlan(int M, int tab_bytes, int H, int L, int max_m, int W, int k, int dim) {
     const size_t C = (size_t)W * max_m;
-    const size_t sz[19] = {4u * (size_t)dim, (size_t)tab_bytes * M * kPivots, 4u * (size_t)H, 4u * (size_t)L,
-                           4u * (size_t)L, 4u * (size_t)L, 4u * (size_t)L, 4 * (C + W), 4 * C, 4 * C, 4 * C,
-                           4 * C, 4 * C, 4u * W, 4u * W, 4u * (size_t)k, 4u * (size_t)k, 64, 4 * C};
+    const size_t sz[17] = {4u * (size_t)dim, (size_t)tab_bytes * M * kPivots, 4u * (size_t)H, 4u * (size_t)L,
+                           4u * (size_t)L, 4 * C, 4 * C, 4 * C, 4 * C, 4 * C, 4 * C, 4u * W, 4u * W,
+                           4u * (size_t)k, 4u * (size_t)k, 64, 4 * C};
     size_t o = 0;
-    for (int i = 0; i < 19; i++) {
+    for (int i = 0; i < 17; i++) {
       off[i] = o;
       o = align16(o + sz[i]);
     }
@@ -68,22 +70,20 @@ __device__ BatchSmem carve_batch(uint8_t* base, const BatchPlan& pl) {
   s.q = (float*)(base + pl.off[0]);
   s.table = base + pl.off[1];
   s.hash = (uint32_t*)(base + pl.off[2]);
-  s.la_id = (uint32_t*)(base + pl.off[3]);
-  s.la_d = (float*)(base + pl.off[4]);
-  s.lb_id = (uint32_t*)(base + pl.off[5]);
-  s.lb_d = (float*)(base + pl.off[6]);
-  s.c_id = (uint32_t*)(base + pl.off[7]);
-  s.c_d = (float*)(base + pl.off[8]);
-  s.s_id = (uint32_t*)(base + pl.off[9]);
-  s.s_d = (float*)(base + pl.off[10]);
-  s.s_lb = (int32_t*)(base + pl.off[11]);
-  s.s_slb = (int32_t*)(base + pl.off[12]);
-  s.sel_id = (int32_t*)(base + pl.off[13]);
-  s.sel_d = (float*)(base + pl.off[14]);
-  s.topk_id = (int32_t*)(base + pl.off[15]);
-  s.topk_d = (float*)(base + pl.off[16]);
-  s.ctrl = (int*)(base + pl.off[17]);
-  s.wnew = (uint32_t*)(base + pl.off[18]);
+  s.l_id = (uint32_t*)(base + pl.off[3]);
+  s.l_d = (float*)(base + pl.off[4]);
+  s.c_id = (uint32_t*)(base + pl.off[5]);
+  s.c_d = (float*)(base + pl.off[6]);
+  s.s_id = (uint32_t*)(base + pl.off[7]);
+  s.s_d = (float*)(base + pl.off[8]);
+  s.s_lb = (int32_t*)(base + pl.off[9]);
+  s.s_slb = (int32_t*)(base + pl.off[10]);
+  s.sel_id = (int32_t*)(base + pl.off[11]);
+  s.sel_d = (float*)(base + pl.off[12]);
+  s.topk_id = (int32_t*)(base + pl.off[13]);
+  s.topk_d = (float*)(base + pl.off[14]);
+  s.ctrl = (int*)(base + pl.off[15]);
+  s.wnew = (uint32_t*)(base + pl.off[16]);
   return s;
 }
 
@@ -117,6 +117,107 @@ __device__ __forceinline__ float adc_split4(const TabT* table, const uint8_t* co
   const float s0 = quarter_sum(table, code, 0, q), s1 = quarter_sum(table, code, q, q);
   const float s2 = quarter_sum(table, code, 2 * q, q), s3 = quarter_sum(table, code, 3 * q, q);
   return (s0 + s1) + (s2 + s3);
+}
+
+// The same sum for M == 32 from the code's two 16-byte words, loaded ahead:
+// quarters are words {0,1}, {2,3}, {4,5}, {6,7}, bytes in chunk order.
+template <class TabT>
+__device__ __forceinline__ float adc32_words(const TabT* table, const uint4& a, const uint4& b) {
+  const uint32_t w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+  float s[4];
+#pragma unroll
+  for (int qq = 0; qq < 4; qq++) {
+    float d = 0.0f;
+#pragma unroll
+    for (int t = 0; t < 2; t++) {
+      const uint32_t x = w[qq * 2 + t];
+      const int c = (qq * 2 + t) * 4;
+      d += load_tab(table, c * kPivots + (x & 0xffu));
+      d += load_tab(table, (c + 1) * kPivots + ((x >> 8) & 0xffu));
+      d += load_tab(table, (c + 2) * kPivots + ((x >> 16) & 0xffu));
+      d += load_tab(table, (c + 3) * kPivots + (x >> 24));
+    }
+    s[qq] = d;
+  }
+  return (s[0] + s[1]) + (s[2] + s[3]);
+}
+
+// Insert up to N (distance, id) pairs, given in push order in vd/vi[0, n),
+// into the sorted top-k (td, ti, size) in one pass of one warp. Pairs with an
+// infinite distance are skipped. The result equals n calls of topk_push in
+// order: a new pair goes after existing entries with an equal distance, and
+// after earlier new pairs with an equal distance.
+template <int N>
+__device__ __forceinline__ void topk_push_many(float* td, int32_t* ti, int& size, int k, const float* vd,
+                                               const int32_t* vi, int n, int lane) {
+  float cd[N];
+  bool cv[N];
+#pragma unroll
+  for (int j = 0; j < N; j++) {
+    cd[j] = j < n ? vd[j] : inf_f();
+    cv[j] = j < n && cd[j] != inf_f();
+  }
+  int nv = 0;
+#pragma unroll
+  for (int j = 0; j < N; j++) nv += cv[j];
+  if (nv == 0) return;
+  if (size == k) {  // full: only a pair below the k-th distance can enter
+    const float worst = td[k - 1];
+    bool any = false;
+#pragma unroll
+    for (int j = 0; j < N; j++) any |= cv[j] && cd[j] < worst;
+    if (!any) return;
+  }
+  float my_d = inf_f();
+  int32_t my_id = 0;
+  bool mine = false;
+  int pos = 0;  // final position of pair `lane` (lane < n)
+#pragma unroll
+  for (int j = 0; j < N; j++) {
+    if (lane == j && cv[j]) {
+      mine = true;
+      my_d = cd[j];
+      my_id = vi[j];
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < N; j++) pos += cv[j] && (cd[j] < my_d || (cd[j] == my_d && j < lane));
+  for (int base = 0; base < size; base += 32) {
+    const int i = base + lane;
+    const float e = i < size ? td[i] : inf_f();
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+      const int c = __popc(__ballot_sync(kFull, i < size && e <= cd[j]));
+      if (lane == j) pos += c;
+    }
+  }
+  const bool enters = mine && pos < k;
+  if (__ballot_sync(kFull, enters)) {
+    for (int c = (size - 1) >> 5; c >= 0; c--) {  // existing entries move up, top chunk first
+      const int i = c * 32 + lane;
+      float e = 0.0f;
+      int32_t eid = 0;
+      int sh = 0;
+      if (i < size) {
+        e = td[i];
+        eid = ti[i];
+#pragma unroll
+        for (int j = 0; j < N; j++) sh += cv[j] && cd[j] < e;
+      }
+      __syncwarp();
+      if (i < size && i + sh < k) {
+        td[i + sh] = e;
+        ti[i + sh] = eid;
+      }
+      __syncwarp();
+    }
+    if (enters) {
+      td[pos] = my_d;
+      ti[pos] = my_id;
+    }
+    __syncwarp();
+  }
+  size = min(size + nv, k);
 }
 
 // Exact squared L2 of the node (its first kVecRegs*32 elements preloaded in
@@ -168,17 +269,51 @@ __device__ void copy_table(void* dst, const __nv_bfloat16* src, int bytes, int t
   for (int i = tid; i < bytes / 16; i += nthreads) d[i] = __ldg(s + i);
 }
 
+constexpr int kStage = 4;  // list entries per thread staged in registers by the in-place merge
+
+// The node's record as one warp holds it: degree, the first kEdgeRegs * 32
+// neighbour slots and kVecRegs * 32 vector elements, loaded in one round trip.
+template <class T>
+struct Record {
+  int64_t u = -1;
+  bool uok = false;
+  const uint8_t* node = nullptr;
+  const int32_t* meta = nullptr;
+  int deg = 0;
+  int ev[kEdgeRegs];
+  float vx[kVecRegs];
+  __device__ __forceinline__ void load(const BatchParams& p, int64_t id, int lane) {
+    u = id;
+    uok = id >= 0 && id < p.n;
+    const uint32_t uu = uok ? (uint32_t)id : 0u;
+    const uint32_t pg = p.npp_div.div(uu);
+    node = p.ix.pages + (int64_t)pg * kPageSize + (int64_t)(uu - pg * (uint32_t)p.npp) * p.node_len;
+    meta = reinterpret_cast<const int32_t*>(node + p.data_len);
+    deg = __ldg(meta);
+#pragma unroll
+    for (int r = 0; r < kEdgeRegs; r++) ev[r] = lane + 32 * r < p.max_m ? __ldg(meta + 1 + lane + 32 * r) : -1;
+#pragma unroll
+    for (int r = 0; r < kVecRegs; r++)
+      vx[r] = lane + 32 * r < p.dim ? load_elem<T>(reinterpret_cast<const T*>(node), lane + 32 * r) : 0.0f;
+  }
+};
+
 template <class T, class TabT, int W>
-__global__ void __launch_bounds__(W * 32, (W <= 4 ? 8 : 4)) batch_search_kernel(BatchParams p) {
+__global__ void __launch_bounds__(W * 32, 24 / W) batch_search_kernel(BatchParams p) {
+  constexpr int NT = W * 32;
+  constexpr int TKW = W - 1;  // warp that marks the picks and keeps the top-k
   extern __shared__ __align__(16) uint8_t smem[];
   const BatchPlan pl(p.M, (int)sizeof(TabT), 1 << p.hash_bits, p.L_max, p.max_m, W, p.k_max, p.dim);
   const BatchSmem s = carve_batch(smem, pl);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int dim = p.dim, M = p.M, H = 1 << p.hash_bits;
+  const bool m32 = M == 32;
   TabT* table = reinterpret_cast<TabT*>(s.table);
   const NavView nv{p.ix.nav_data, p.ix.nav_graph, p.ix.nav_map, p.nav_n, p.nav_max_m, p.nav_start, dim, p.fma,
                    p.err};
   const PqView pv{p.ix.pivots_t, p.ix.centroid, p.ix.chunk_off, M, dim, p.fma};
+  uint32_t* const list_id = s.l_id;
+  float* const list_d = s.l_d;
 
   for (;;) {
     if (tid == 0) s.ctrl[0] = atomicAdd(p.next_query, 1);
@@ -187,8 +322,8 @@ __global__ void __launch_bounds__(W * 32, (W <= 4 ? 8 : 4)) batch_search_kernel(
     if (qid >= p.nq) break;
     const int L = p.L_per_q ? min(max(__ldg(p.L_per_q + qid), 1), p.L_max) : p.L_max;
     const int k = p.k_per_q ? min(max(__ldg(p.k_per_q + qid), 1), p.k_max) : p.k_max;
-    for (int i = tid; i < dim; i += W * 32) s.q[i] = __ldg(p.queries + (size_t)qid * dim + i);
-    for (int i = tid; i < H; i += W * 32) s.hash[i] = 0xffffffffu;
+    for (int i = tid; i < dim; i += NT) s.q[i] = __ldg(p.queries + (size_t)qid * dim + i);
+    for (int i = tid; i < H; i += NT) s.hash[i] = 0xffffffffu;
     __syncthreads();
     int64_t gathered = 0;  // per-warp share of the algorithmic bytes
     if (warp == 0) {
@@ -196,7 +331,7 @@ __global__ void __launch_bounds__(W * 32, (W <= 4 ? 8 : 4)) batch_search_kernel(
       if (lane == 0) s.ctrl[3] = (int)u0;
     }
     if (p.tables) {  // BF16 tables built for the whole batch on the tensor cores
-      copy_table(s.table, p.tables + (size_t)qid * M * kPivots, M * kPivots * 2, tid, W * 32);
+      copy_table(s.table, p.tables + (size_t)qid * M * kPivots, M * kPivots * 2, tid, NT);
     } else if (W == 1) {
       build_table(pv, table, s.q, 0, 1, lane);
     } else if (warp > 0) {
@@ -207,7 +342,7 @@ __global__ void __launch_bounds__(W * 32, (W <= 4 ? 8 : 4)) batch_search_kernel(
     // reproduce that rounding). uint8 data with integral queries take the
     // int32 path.
     bool iq = sizeof(T) == 1;
-    for (int i = tid; i < dim && iq; i += W * 32) iq = s.q[i] == rintf(s.q[i]) && s.q[i] >= 0.0f && s.q[i] <= 255.0f;
+    for (int i = tid; i < dim && iq; i += NT) iq = s.q[i] == rintf(s.q[i]) && s.q[i] >= 0.0f && s.q[i] <= 255.0f;
     const bool int_query = __syncthreads_and(iq) != 0;
     // The entry node starts the list, unexpanded, with its ADC distance; the
     // first step picks it (the reference expands it without listing it,
@@ -216,64 +351,74 @@ __global__ void __launch_bounds__(W * 32, (W <= 4 ? 8 : 4)) batch_search_kernel(
     // the visited cache holds.
     const int u0 = s.ctrl[3];
     if (tid == 0) {
-      s.ctrl[2] = 0;  // survivors of the current step
-      s.ctrl[4] = 0;  // a repeated id among them
-      s.ctrl[6] = 0;  // stop (hop limit)
+      s.ctrl[2] = 0;        // survivors of the current step
+      s.ctrl[4] = 0;        // a repeated id among them
+      s.ctrl[6] = 0;        // stop (hop limit)
+      s.ctrl[7] = INT_MAX;  // first insertion point of the current step
       if (u0 >= 0) {
         s.hash[hash_slot((uint32_t)u0, p.hash_bits)] = (uint32_t)u0;
-        s.la_id[0] = (uint32_t)u0;
-        s.la_d[0] = adc_split4(table, p.ix.codes + (size_t)u0 * M, M);
+        list_id[0] = (uint32_t)u0;
+        const uint8_t* code = p.ix.codes + (size_t)u0 * M;
+        list_d[0] = m32 ? adc32_words(table, __ldg(reinterpret_cast<const uint4*>(code)),
+                                      __ldg(reinterpret_cast<const uint4*>(code) + 1))
+                        : adc_split4(table, code, M);
       }
     }
     __syncthreads();
 
-    // List state, identical in every thread; top-k state in warp 0.
-    int sz = u0 >= 0 ? 1 : 0, found = 0, hops = 0, scan_from = 0;
-    uint32_t* list_id = s.la_id;
-    float* list_d = s.la_d;
-    uint32_t* out_id = s.lb_id;
-    float* out_d = s.lb_d;
+    // List state, identical in every thread; top-k state in warp TKW. The
+    // picks of a step (the first W unexpanded entries of the list) are known
+    // when the step starts: the first step picks the entry, and each step
+    // works out the next step's picks from the sorted survivors before it
+    // rewrites the list, so that each warp's next record is already on its
+    // way while the list is merged.
+    int sz = u0 >= 0 ? 1 : 0, found = 0, hops = 0;
+    int npick = u0 >= 0 ? 1 : 0, last_pos = 0;
+    int pick_pos[W];
+#pragma unroll
+    for (int w = 0; w < W; w++) pick_pos[w] = w == 0 && u0 >= 0 ? 0 : -1;
+    Record<T> rec;
+    if (warp == 0 && u0 >= 0) rec.load(p, u0, lane);
 
     for (;;) {
-      // Pick: every warp finds the same first W unexpanded entries (entries
-      // before scan_from are expanded and have not moved) and takes its own.
-      int npick = 0, my_pos = -1;
-      for (int base = scan_from; base < sz && npick < W; base += 32) {
-        const int i = base + lane;
-        unsigned um = __ballot_sync(kFull, i < sz && !(list_id[i] & kExpanded));
-        if (base == scan_from && um == 0) scan_from = min(base + 32, sz);
-        while (um && npick < W) {
-          const int b = __ffs(um) - 1;
-          um &= um - 1;
-          if (npick == warp) my_pos = base + b;
-          npick++;
-        }
-      }
       if (npick == 0 || s.ctrl[6]) break;
       const bool full = sz == L;
       const float tail_d = full ? list_d[L - 1] : 0.0f;
       const uint32_t tail_id = full ? list_id[L - 1] : 0u;
-      // Expand: warp w expands pick w. The degree word, the neighbour slots
-      // (up to max_m, inside the record) and the node's vector are loaded
-      // together, so the record costs one memory round trip. New neighbours
-      // are scored and checked against the list here; survivors (below the
-      // list's last key when it is full, not in it yet) are kept unsorted.
+      // Old candidates for the next step: the first W unexpanded entries after
+      // the last pick (every unexpanded entry before it is a pick). Lane t < W
+      // holds candidate t; every warp holds the same.
+      int noc = 0, oc_pos = INT_MAX;
+      uint32_t oc_id = 0;
+      for (int base = last_pos + 1; base < sz && noc < W; base += 32) {
+        const int i = base + lane;
+        const uint32_t id = i < sz ? list_id[i] : kExpanded;
+        const bool un = !(id & kExpanded);
+        const unsigned um = __ballot_sync(kFull, un);
+        const int g = noc + __popc(um & ((1u << lane) - 1));  // candidate index of an unexpanded entry
+#pragma unroll
+        for (int t = 0; t < W; t++) {
+          const unsigned sel = __ballot_sync(kFull, un && g == t);
+          if (sel) {
+            const int srcl = __ffs(sel) - 1;
+            const uint32_t cid = __shfl_sync(kFull, id, srcl);
+            if (lane == t) {
+              oc_pos = base + srcl;
+              oc_id = cid & kMask;
+            }
+          }
+        }
+        noc = min(W, noc + __popc(um));
+      }
+      // Expand: warp w expands pick w (its record was loaded when the pick was
+      // made). New neighbours are scored and checked against the list here;
+      // survivors (below the list's last key when it is full, not in it yet)
+      // are kept unsorted.
       if (warp < npick) {
-        const int64_t u = list_id[my_pos] & kMask;
-        const bool uok = u < p.n;
-        const uint8_t* node = p.ix.pages + (uok ? (u / p.npp) * kPageSize + (u % p.npp) * p.node_len : 0);
-        const int32_t* meta = reinterpret_cast<const int32_t*>(node + p.data_len);
-        int deg = __ldg(meta);
-        int ev[kEdgeRegs];
-#pragma unroll
-        for (int r = 0; r < kEdgeRegs; r++) ev[r] = lane + 32 * r < p.max_m ? __ldg(meta + 1 + lane + 32 * r) : -1;
-        float vx[kVecRegs];
-#pragma unroll
-        for (int r = 0; r < kVecRegs; r++)
-          vx[r] = lane + 32 * r < dim ? load_elem<T>(reinterpret_cast<const T*>(node), lane + 32 * r) : 0.0f;
-        const bool ok = uok && deg >= 0 && deg <= p.max_m;
+        const bool ok = rec.uok && rec.deg >= 0 && rec.deg <= p.max_m;
+        int deg = rec.deg;
         if (!ok) {
-          if (lane == 0) atomicOr(p.err, uok ? kErrBadDegree : kErrBadId);
+          if (lane == 0) atomicOr(p.err, rec.uok ? kErrBadDegree : kErrBadId);
           deg = 0;
         }
         // Visited-cache check of every neighbour; the new ones are compacted
@@ -293,9 +438,9 @@ __global__ void __launch_bounds__(W * 32, (W <= 4 ? 8 : 4)) batch_search_kernel(
           nnew += __popc(m);
         };
 #pragma unroll
-        for (int r = 0; r < kEdgeRegs; r++) check(lane + 32 * r, ev[r]);
+        for (int r = 0; r < kEdgeRegs; r++) check(lane + 32 * r, rec.ev[r]);
         for (int b0 = 32 * kEdgeRegs; b0 < deg; b0 += 32)
-          check(b0 + lane, b0 + lane < deg ? __ldg(meta + 1 + b0 + lane) : -1);
+          check(b0 + lane, b0 + lane < deg ? __ldg(rec.meta + 1 + b0 + lane) : -1);
         __syncwarp();
         // Score the new ones and keep the survivors: below the list's last key
         // when it is full, not in it yet.
@@ -307,32 +452,44 @@ __global__ void __launch_bounds__(W * 32, (W <= 4 ? 8 : 4)) batch_search_kernel(
           s.s_id[slot] = v;
           s.s_d[slot] = d;
           s.s_lb[slot] = lb;
+          atomicMin(&s.ctrl[7], lb);
         };
         // One lane per new neighbour: all of the warp's code fetches are in
-        // flight at once, and no lane runs a second ADC while others idle.
-        for (int i = lane; i < nnew; i += 32) {
+        // flight at once (for M == 32 as two 16-byte loads issued before the
+        // exact distance), and no lane runs a second ADC while others idle.
+        const bool has = lane < nnew;
+        const uint32_t v0 = has ? wnew[lane] : 0u;
+        uint4 cw0 = make_uint4(0, 0, 0, 0), cw1 = cw0;
+        if (has && m32) {
+          const uint4* c4 = reinterpret_cast<const uint4*>(p.ix.codes + (size_t)v0 * 32);
+          cw0 = __ldg(c4);
+          cw1 = __ldg(c4 + 1);
+        }
+        float ed = inf_f();
+        if (ok) ed = exact_dist<T>(s.q, reinterpret_cast<const T*>(rec.node), rec.vx, dim, lane, int_query, p.fma);
+        if (has) keep(v0, m32 ? adc32_words(table, cw0, cw1) : adc_split4(table, p.ix.codes + (size_t)v0 * M, M));
+        for (int i = lane + 32; i < nnew; i += 32) {
           const uint32_t v = wnew[i];
           keep(v, adc_split4(table, p.ix.codes + (size_t)v * M, M));
         }
-        const int scored = lane == 0 ? nnew : 0;
-        float ed = inf_f();
-        if (ok) ed = exact_dist<T>(s.q, reinterpret_cast<const T*>(node), vx, dim, lane, int_query, p.fma);
         if (lane == 0) {
           s.sel_d[warp] = ed;
-          s.sel_id[warp] = (int32_t)u;
-          s.c_id[warp] = (uint32_t)my_pos;  // list position of the pick (marked below)
+          s.sel_id[warp] = (int32_t)rec.u;
         }
-        const int sc = __reduce_add_sync(kFull, scored);
-        gathered += ok ? 4 + 4 * deg + p.data_len + (int64_t)sc * M : 0;
+        gathered += ok ? 4 + 4 * deg + p.data_len + (int64_t)nnew * M : 0;
       }
-      __syncthreads();  // (1) survivors and picks are in
+      __syncthreads();  // (1) survivors and exact distances are in
       const int nsv = s.ctrl[2];
-      if (warp == 0) {  // mark the picks, keep the top-k
-        for (int w = 0; w < npick; w++) {
-          if (lane == 0) list_id[s.c_id[w]] |= kExpanded;
-          if (s.sel_d[w] != inf_f()) topk_push(s.topk_d, s.topk_id, found, k, s.sel_d[w], s.sel_id[w], lane);
-          hops++;
-        }
+      const int first_new = s.ctrl[7];  // INT_MAX when nothing survived
+      // The merge's first round covers [lo1, sz); a pick there is marked when
+      // it is staged, every other pick in place.
+      const int lo1 = min(sz, max(first_new, sz - kStage * NT));
+      if (warp == TKW) {  // mark the picks outside the first round, keep the top-k
+#pragma unroll
+        for (int w = 0; w < W; w++)
+          if (lane == w && w < npick && pick_pos[w] < lo1) list_id[pick_pos[w]] |= kExpanded;
+        topk_push_many<W>(s.topk_d, s.topk_id, found, k, s.sel_d, s.sel_id, npick, lane);
+        hops += npick;
         if (lane == 0 && hops > kHopCap) {
           s.ctrl[6] = 1;
           atomicOr(p.err, kErrHopCap);
@@ -340,25 +497,57 @@ __global__ void __launch_bounds__(W * 32, (W <= 4 ? 8 : 4)) batch_search_kernel(
       }
       // Rank-sort the survivors (rank = number of smaller keys, ties by slot);
       // a repeated id (a cache eviction between two lookups) raises a flag.
-      for (int j = tid; j < nsv; j += W * 32) {
-        const float d = s.s_d[j];
-        const uint32_t id = s.s_id[j];
-        int r = 0;
-        bool rep = false;
-        for (int f = 0; f < nsv; f++) {
-          const float fd = s.s_d[f];
-          const uint32_t fi = s.s_id[f];
-          const bool same = fd == d && ((fi ^ id) & kMask) == 0;
-          r += key_less(fd, fi, d, id) || (same && f < j);
-          rep |= same && f != j;
+      // Warp TKW is busy with the top-k, so the other warps sort.
+      if (W == 1 || warp != TKW) {
+        constexpr int RS = W == 1 ? 32 : NT - 32;
+        for (int j = tid; j < nsv; j += RS) {
+          const float d = s.s_d[j];
+          const uint32_t id = s.s_id[j];
+          int r = 0;
+          bool rep = false;
+          for (int f = 0; f < nsv; f++) {
+            const float fd = s.s_d[f];
+            const uint32_t fi = s.s_id[f];
+            const bool same = fd == d && ((fi ^ id) & kMask) == 0;
+            r += key_less(fd, fi, d, id) || (same && f < j);
+            rep |= same && f != j;
+          }
+          s.c_id[r] = id;  // sorted survivors
+          s.c_d[r] = d;
+          s.s_slb[r] = s.s_lb[j];
+          if (rep) s.ctrl[4] = 1;
         }
-        s.c_id[W + r] = id;  // sorted survivors after the W pick slots
-        s.c_d[r] = d;
-        s.s_slb[r] = s.s_lb[j];
-        if (rep) s.ctrl[4] = 1;
       }
+      // In-place merge. Entries from the first insertion point on move up:
+      // old entry i goes to i + #{survivors inserted at or before i}, survivor
+      // r to its insertion point + r; positions >= L drop. Each round stages
+      // the top kStage * NT entries still to move in registers, waits for
+      // every thread, then writes; the first round's wait is barrier (2)
+      // (a pick staged there takes its expanded mark with it), and survivors
+      // are written after the last round.
+      uint32_t st_id[kStage];
+      float st_d[kStage];
+      int hi = sz;
+      auto round_lo = [&]() { return min(hi, max(first_new, hi - kStage * NT)); };
+      auto stage = [&](bool first) {
+        const int lo = round_lo();
+#pragma unroll
+        for (int r = 0; r < kStage; r++) {
+          const int i = lo + r * NT + tid;
+          if (i < hi) {
+            uint32_t id = list_id[i];
+            if (first) {
+#pragma unroll
+              for (int w = 0; w < W; w++) id |= pick_pos[w] == i ? kExpanded : 0u;
+            }
+            st_id[r] = id;
+            st_d[r] = list_d[i];
+          }
+        }
+      };
+      stage(true);
       __syncthreads();  // (2)
-      uint32_t* sid = s.c_id + W;
+      uint32_t* const sid = s.c_id;
       int ns = nsv;
       const bool repeated = s.ctrl[4] != 0;
       if (repeated) {  // rare: drop repeated ids (warp 0), then share the count
@@ -392,49 +581,91 @@ __global__ void __launch_bounds__(W * 32, (W <= 4 ? 8 : 4)) batch_search_kernel(
         __syncthreads();
         ns = s.ctrl[5];
       }
-      // Move old entries and survivors into the other list buffer: old entry i
-      // goes to i + #{survivors inserted at or before i}, survivor r to its
-      // insertion point + r; positions >= L drop.
-      const int nsz = min(sz + ns, L);
-      if (ns) {
-        for (int i = tid; i < sz; i += W * 32) {
-          int lo = 0, hi = ns;
-          while (lo < hi) {
-            const int mid = (lo + hi) >> 1;
-            if (s.s_slb[mid] <= i) lo = mid + 1; else hi = mid;
+      // Next picks: the first W of the old candidates and the first W
+      // survivors by position in the merged list, below L. Lane t < W holds
+      // old candidate t, lane W + r survivor r; every warp computes the same.
+      {
+        int mpos = INT_MAX;
+        uint32_t mid = 0;
+        if (lane < W && lane < noc) {
+          int lo = 0, up = ns;
+          while (lo < up) {
+            const int md = (lo + up) >> 1;
+            if (s.s_slb[md] <= oc_pos) lo = md + 1; else up = md;
           }
-          const int dst = i + lo;
-          if (dst < L) {
-            out_id[dst] = list_id[i];
-            out_d[dst] = list_d[i];
-          }
+          mpos = oc_pos + lo;
+          mid = oc_id;
+        } else if (lane >= W && lane < 2 * W && lane - W < ns) {
+          mpos = s.s_slb[lane - W] + (lane - W);
+          mid = sid[lane - W] & kMask;
         }
-        for (int r = tid; r < ns; r += W * 32) {
+        if (mpos >= L) mpos = INT_MAX;
+        int rank = 0;  // among the valid entries (their positions are distinct)
+#pragma unroll
+        for (int j = 0; j < 2 * W; j++) rank += __shfl_sync(kFull, mpos, j) < mpos;
+        const bool take = mpos != INT_MAX && rank < W;
+        npick = __popc(__ballot_sync(kFull, take));
+        uint32_t my_next = 0;
+#pragma unroll
+        for (int w = 0; w < W; w++) {
+          const unsigned sel = __ballot_sync(kFull, take && rank == w);
+          const int srcl = sel ? __ffs(sel) - 1 : 0;
+          const int ppos = __shfl_sync(kFull, mpos, srcl);
+          const uint32_t pid = __shfl_sync(kFull, mid, srcl);
+          pick_pos[w] = sel ? ppos : -1;
+          if (sel) last_pos = ppos;
+          if (w == warp) my_next = pid;
+        }
+        if (warp < npick) rec.load(p, (int64_t)my_next, lane);
+      }
+      if (ns) {
+        for (;;) {
+          const int lo = round_lo();
+#pragma unroll
+          for (int r = 0; r < kStage; r++) {
+            const int i = lo + r * NT + tid;
+            if (i < hi) {
+              int a = 0, b = ns;
+              while (a < b) {
+                const int md = (a + b) >> 1;
+                if (s.s_slb[md] <= i) a = md + 1; else b = md;
+              }
+              const int dst = i + a;
+              if (dst < L) {
+                list_id[dst] = st_id[r];
+                list_d[dst] = st_d[r];
+              }
+            }
+          }
+          hi = lo;
+          if (hi <= first_new) break;
+          stage(false);
+          __syncthreads();
+        }
+        // Every old entry was read before a barrier that precedes this point,
+        // and survivors and old entries land on distinct positions.
+        for (int r = tid; r < ns; r += NT) {
           const int dst = s.s_slb[r] + r;
           if (dst < L) {
-            out_id[dst] = sid[r];
-            out_d[dst] = s.c_d[r];
+            list_id[dst] = sid[r];
+            list_d[dst] = s.c_d[r];
           }
         }
-        const int first_new = s.s_slb[0];
-        if (first_new < scan_from) scan_from = first_new;
-        uint32_t* ti = list_id;
-        float* td = list_d;
-        list_id = out_id;
-        list_d = out_d;
-        out_id = ti;
-        out_d = td;
       }
-      sz = nsz;
-      // Every thread read the survivor count after (1); the next step adds to
-      // it only after (3), so it is reset here. The repeat flag is read by every
-      // thread after (2) and set again only after the next (1).
-      if (tid == 0) s.ctrl[2] = 0;
+      sz = min(sz + ns, L);
+      // Every thread read the survivor count and the first insertion point
+      // after (1); the next step adds to them only after (3), so they are
+      // reset here. The repeat flag is read by every thread after (2) and set
+      // again only after the next (1).
+      if (tid == 0) {
+        s.ctrl[2] = 0;
+        s.ctrl[7] = INT_MAX;
+      }
       __syncthreads();  // (3) the new list is complete
       if (tid == 0) s.ctrl[4] = 0;
     }
-    // outputs (warp 0 holds the top-k bookkeeping)
-    if (warp == 0) {
+    // outputs (warp TKW holds the top-k bookkeeping)
+    if (warp == TKW) {
       const size_t row = (size_t)qid * p.k_max;
       for (int i = lane; i < p.k_max; i += 32) {
         p.nns[row + i] = i < found ? s.topk_id[i] : 0;
