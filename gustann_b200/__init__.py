@@ -105,6 +105,9 @@ _SIGNATURES = {
     "gann_search_batch": (_I, [_P, _P, _I, _P, _P, _I, _I, _P, _P, _P, _P, ctypes.POINTER(ctypes.c_double)]),
     "gann_search_batch_device": (_I, [_P, _P, _I, _P, _P, _I, _I, _P, _P, _P, _P, _P, _P, _P]),
     "gann_search_batch_noalloc": (_I, [_P, _P, _I, _I, _I, _P, _P, _P, _P, _P]),
+    "gann_batch_graph_create": (_I, [_P, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P, ctypes.POINTER(_P)]),
+    "gann_batch_graph_launch": (_I, [_P, _P]),
+    "gann_batch_graph_destroy": (_I, [_P]),
     "gann_pq_tables": (_I, [_P, _P, _I, _I, _P]),
     "gann_autotune": (_I, [_P, _P, _I, _I, _I, _I, _P, ctypes.POINTER(ctypes.c_double)]),
     "gann_server_start": (_I, [_P, ctypes.POINTER(ServerOpts), ctypes.POINTER(_P)]),
@@ -309,6 +312,36 @@ class GustANN:
     def __del__(self):
         try:
             self.close()
+        except Exception:
+            pass
+
+
+class BatchGraph:
+    """A batched search captured once as a CUDA graph (gann_batch_graph_*).
+    The device buffers (ints are device addresses) are fixed at capture; each
+    launch processes the number of queries held in the device int at ``d_nq``."""
+
+    def __init__(self, index: GustANN, max_nq: int, topk_max: int, ef_max: int, d_q: int, d_nq: int, d_nns: int,
+                 d_dists: int, d_found: int, d_topk: int = 0, d_ef: int = 0, precision: int = PREC_BF16,
+                 beam_width: int = 0, hash_bits: int = 0):
+        self.index = index
+        o = index._opts(precision, beam_width, hash_bits)
+        self._g = _P()
+        _check(lib().gann_batch_graph_create(index.handle, max_nq, topk_max, ef_max, ctypes.byref(o), d_q,
+                                             d_topk or None, d_ef or None, d_nq, d_nns, d_dists, d_found,
+                                             ctypes.byref(self._g)))
+
+    def launch(self, stream: int | None = None) -> None:
+        _check(lib().gann_batch_graph_launch(self._g, _stream(stream)))
+
+    def destroy(self) -> None:
+        if self._g:
+            lib().gann_batch_graph_destroy(self._g)
+            self._g = None
+
+    def __del__(self):
+        try:
+            self.destroy()
         except Exception:
             pass
 

@@ -431,7 +431,7 @@ int batch_hash_bits(int ef_max) {
 int enqueue_batch(gann_t* h, const float* d_q, int nq, const int32_t* d_k, const int32_t* d_l, int k_max,
                   int l_max, const gann_batch_opts_t* opts, int32_t* d_nns, float* d_dists, int32_t* d_found,
                   int32_t* d_hops, int64_t* d_bytes, cudaStream_t s, int* counter = nullptr,
-                  __nv_bfloat16* tables = nullptr) {
+                  __nv_bfloat16* tables = nullptr, const int* nq_dev = nullptr) {
   gann_batch_opts_t o{};
   if (opts) o = *opts;
   const int prec = opts ? o.precision : GANN_PREC_BF16;
@@ -461,6 +461,7 @@ int enqueue_batch(gann_t* h, const float* d_q, int nq, const int32_t* d_k, const
   p.nav_start = h->hx.nav_start;
   p.queries = d_q;
   p.nq = nq;
+  p.nq_dev = nq_dev;
   p.L_per_q = d_l;
   p.k_per_q = d_k;
   p.L_max = l_max;
@@ -489,7 +490,7 @@ int enqueue_batch(gann_t* h, const float* d_q, int nq, const int32_t* d_k, const
       h->cap_tables = need;
     }
     __nv_bfloat16* tab = tables ? tables : h->d_tables;
-    e = gann::launch_table_tc(h->dx, (int)h->hx.dim, h->hx.pq_m, d_q, nq, prec == GANN_PREC_BF16X3, tab, s);
+    e = gann::launch_table_tc(h->dx, (int)h->hx.dim, h->hx.pq_m, d_q, nq, prec == GANN_PREC_BF16X3, tab, s, nq_dev);
     if (e != cudaSuccess) return set_error(GANN_ECUDA, std::string("table build: ") + cudaGetErrorString(e));
     p.tables = tab;
   }
@@ -724,12 +725,14 @@ int gann_set_fma(gann_t* h, int fma_table, int fma_exact) {
 
 }  // extern "C"
 
-// Batched launch with caller-owned counter and tables (the server's batch slots).
-int gann_internal_enqueue_batch(gann_t* h, const float* d_q, int nq, const int32_t* d_k, const int32_t* d_l,
-                                int k_max, int l_max, const gann_batch_opts_t* opts, int32_t* d_nns,
-                                float* d_dists, int32_t* d_found, cudaStream_t s, int* counter,
-                                __nv_bfloat16* tables) {
+// A batched search on device buffers with a caller-owned counter and tables;
+// the query count is read at run time from device memory when nq_dev is set
+// (batch_graph.cu).
+int gann_internal_enqueue_batch_dev(gann_t* h, const float* d_q, int nq, const int32_t* d_k, const int32_t* d_l,
+                                    int k_max, int l_max, const gann_batch_opts_t* opts, int32_t* d_nns,
+                                    float* d_dists, int32_t* d_found, cudaStream_t s, int* counter,
+                                    __nv_bfloat16* tables, const int* nq_dev) {
   return enqueue_batch(h, d_q, nq, d_k, d_l, k_max, l_max, opts, d_nns, d_dists, d_found, nullptr, nullptr, s,
-                       counter, tables);
+                       counter, tables, nq_dev);
 }
 

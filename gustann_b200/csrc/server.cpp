@@ -6,7 +6,10 @@
 // and launches it on that slot's stream, so requests that arrive while others
 // run on the GPU start as soon as a slot frees up, and up to `streams` batches
 // overlap on the device. Each slot owns its device buffers (queries, per-query
-// k and L, results, work counter, BF16 tables), allocated at start; admission
+// k and L, the batch size, results) and a CUDA graph of the batched search
+// captured over them at start (gann_batch_graph_create: counter reset, table
+// build, persistent walk reading the batch size from device memory), so a
+// batch is its input copies, one graph launch and its output copies. Admission
 // is by that budget: a submit is refused (GANN_EBUSY) while every request slot
 // of the server is taken. Per-query state (candidate list, visited cache,
 // table) lives on the device for the life of its batch. A request's result
@@ -25,10 +28,6 @@
 #include "gann_internal.h"
 
 int gann_internal_set_error(int code, const char* msg);
-int gann_internal_enqueue_batch(gann_t* h, const float* d_q, int nq, const int32_t* d_k, const int32_t* d_l,
-                                int k_max, int l_max, const gann_batch_opts_t* opts, int32_t* d_nns,
-                                float* d_dists, int32_t* d_found, cudaStream_t s, int* counter,
-                                __nv_bfloat16* tables);
 
 namespace {
 
@@ -45,8 +44,9 @@ struct Slot {
   float* d_q = nullptr;
   int32_t *d_k = nullptr, *d_l = nullptr, *d_nns = nullptr, *d_f = nullptr;
   float* d_d = nullptr;
-  int* d_counter = nullptr;
-  __nv_bfloat16* d_tab = nullptr;
+  int32_t* h_nq = nullptr;  // batch size (pinned) and its device copy read by the graph
+  int32_t* d_nq = nullptr;
+  gann_batch_graph_t* graph = nullptr;
   std::vector<uint64_t> tags;
   std::vector<double> t_submit;
   int count = 0;
@@ -83,17 +83,19 @@ struct gann_server {
 namespace {
 
 void free_slot(Slot& s) {
-  for (void* p : {(void*)s.h_q, (void*)s.h_k, (void*)s.h_l, (void*)s.h_nns, (void*)s.h_f, (void*)s.h_d})
+  if (s.graph) gann_batch_graph_destroy(s.graph);
+  for (void* p : {(void*)s.h_q, (void*)s.h_k, (void*)s.h_l, (void*)s.h_nns, (void*)s.h_f, (void*)s.h_d,
+                  (void*)s.h_nq})
     if (p) cudaFreeHost(p);
   for (void* p : {(void*)s.d_q, (void*)s.d_k, (void*)s.d_l, (void*)s.d_nns, (void*)s.d_f, (void*)s.d_d,
-                  (void*)s.d_counter, (void*)s.d_tab})
+                  (void*)s.d_nq})
     if (p) cudaFree(p);
   if (s.done) cudaEventDestroy(s.done);
   if (s.stream) cudaStreamDestroy(s.stream);
   s = Slot{};
 }
 
-cudaError_t alloc_slot(Slot& s, int B, int dim, int kmax, int M, bool tables) {
+cudaError_t alloc_slot(Slot& s, int B, int dim, int kmax) {
   cudaError_t e = cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaMallocHost(&s.h_q, sizeof(float) * (size_t)B * dim);
@@ -108,8 +110,8 @@ cudaError_t alloc_slot(Slot& s, int B, int dim, int kmax, int M, bool tables) {
   if (e == cudaSuccess) e = cudaMalloc(&s.d_nns, sizeof(int32_t) * (size_t)B * kmax);
   if (e == cudaSuccess) e = cudaMalloc(&s.d_d, sizeof(float) * (size_t)B * kmax);
   if (e == cudaSuccess) e = cudaMalloc(&s.d_f, sizeof(int32_t) * B);
-  if (e == cudaSuccess) e = cudaMalloc(&s.d_counter, sizeof(int) * 4);
-  if (e == cudaSuccess && tables) e = cudaMalloc(&s.d_tab, sizeof(__nv_bfloat16) * (size_t)B * M * gann::kPivots);
+  if (e == cudaSuccess) e = cudaMallocHost(&s.h_nq, sizeof(int32_t));
+  if (e == cudaSuccess) e = cudaMalloc(&s.d_nq, sizeof(int32_t));
   s.tags.resize(B);
   s.t_submit.resize(B);
   return e;
@@ -186,19 +188,13 @@ bool launch(gann_server* sv) {
   s->busy = true;
   const int kmax = sv->o.topk_max;
   cudaStream_t st = s->stream;
+  *s->h_nq = n;
   cudaError_t e = cudaMemcpyAsync(s->d_q, s->h_q, sizeof(float) * (size_t)n * dim, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(s->d_k, s->h_k, sizeof(int32_t) * n, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(s->d_l, s->h_l, sizeof(int32_t) * n, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(s->d_nq, s->h_nq, sizeof(int32_t), cudaMemcpyHostToDevice, st);
   int rc = GANN_OK;
-  if (e == cudaSuccess) {
-    gann_batch_opts_t bo{};
-    bo.precision = sv->o.precision;
-    bo.beam_width = sv->o.beam_width;
-    bo.hash_bits = sv->o.hash_bits;
-    std::lock_guard<std::mutex> lk(sv->h->mu);
-    rc = gann_internal_enqueue_batch(sv->h, s->d_q, n, s->d_k, s->d_l, kmax, sv->o.ef_max, &bo, s->d_nns, s->d_d,
-                                     s->d_f, st, s->d_counter, s->d_tab);
-  }
+  if (e == cudaSuccess) rc = gann_batch_graph_launch(s->graph, st);
   if (e == cudaSuccess && rc == GANN_OK)
     e = cudaMemcpyAsync(s->h_nns, s->d_nns, sizeof(int32_t) * (size_t)n * kmax, cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess && rc == GANN_OK)
@@ -277,7 +273,6 @@ int gann_server_start(gann_t* h, const gann_server_opts_t* opts, gann_server_t**
   if (o.max_batch < 1 || o.streams < 1 || o.streams > 64 || o.topk_max < 1 || o.ef_max < 1 || o.topk_max > 4096 ||
       o.ef_max > 4096 || o.max_wait_us < 0)
     return gann_internal_set_error(GANN_EINVAL, "bad server options");
-  const bool tables = o.precision == GANN_PREC_BF16 || o.precision == GANN_PREC_BF16X3;
   auto* sv = new gann_server();
   sv->h = h;
   sv->o = o;
@@ -299,15 +294,26 @@ int gann_server_start(gann_t* h, const gann_server_opts_t* opts, gann_server_t**
   cudaGetDevice(&prev);
   cudaSetDevice(h->device);
   cudaError_t e = cudaSuccess;
+  int rc = GANN_OK;
+  gann_batch_opts_t bo{};
+  bo.precision = o.precision;
+  bo.beam_width = o.beam_width;
+  bo.hash_bits = o.hash_bits;
   for (Slot& s : sv->slots) {
-    e = alloc_slot(s, o.max_batch, sv->dim, o.topk_max, sv->M, tables);
+    e = alloc_slot(s, o.max_batch, sv->dim, o.topk_max);
     if (e != cudaSuccess) break;
+    // The slot's batched search, captured over its buffers; the batch size is read from d_nq.
+    rc = gann_batch_graph_create(h, o.max_batch, o.topk_max, o.ef_max, &bo, s.d_q, s.d_k, s.d_l, s.d_nq, s.d_nns,
+                                 s.d_d, s.d_f, &s.graph);
+    if (rc != GANN_OK) break;
   }
   if (prev >= 0) cudaSetDevice(prev);
-  if (e != cudaSuccess) {
+  if (e != cudaSuccess || rc != GANN_OK) {
+    const std::string msg = e != cudaSuccess ? std::string("server buffers: ") + cudaGetErrorString(e)
+                                             : std::string("server batch graph: ") + gann_last_error();
     for (Slot& s : sv->slots) free_slot(s);
     delete sv;
-    return gann_internal_set_error(GANN_ENOMEM, (std::string("server buffers: ") + cudaGetErrorString(e)).c_str());
+    return gann_internal_set_error(e != cudaSuccess ? GANN_ENOMEM : rc, msg.c_str());
   }
   sv->th = std::thread(dispatcher, sv);
   *out = sv;

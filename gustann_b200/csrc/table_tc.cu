@@ -131,6 +131,7 @@ __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::
 struct TcParams {
   const float* queries;      // nq x dim
   int nq, dim, M, p, groups;
+  const int* nq_dev;         // or null: the query count, read at run time (<= nq)
   const float* centroid;     // dim
   const int32_t* chunk_off;  // M + 1
   const uint8_t* bpanel_hi;  // M x 8 KB B tiles
@@ -154,6 +155,11 @@ __global__ void __launch_bounds__(kTile, 1) table_tc_kernel(TcParams p) {
   const int tid = threadIdx.x, warp = tid >> 5;
   const int q0 = blockIdx.x * kTile;
   const int qi = q0 + tid;
+  if (p.nq_dev) {  // tiles past the run-time count leave before taking tensor memory
+    const int n = min(p.nq, *p.nq_dev);
+    if (q0 >= n) return;
+    p.nq = n;
+  }
   const int G = kK / p.p;
   // chunk range of this CTA: whole groups, split over gridDim.y
   const int gpb = (p.groups + gridDim.y - 1) / gridDim.y;
@@ -347,11 +353,12 @@ bool make_tc_panels(const std::vector<float>& pivots, const std::vector<int32_t>
 }
 
 cudaError_t launch_table_tc(const DeviceIndex& ix, int dim, int M, const float* queries, int nq, int split3,
-                            __nv_bfloat16* tables, cudaStream_t stream) {
+                            __nv_bfloat16* tables, cudaStream_t stream, const int* nq_dev) {
   if (!ix.tc_bpanel_hi) return cudaErrorNotSupported;
   TcParams tp{};
   tp.queries = queries;
   tp.nq = nq;
+  tp.nq_dev = nq_dev;
   tp.dim = dim;
   tp.M = M;
   tp.p = ix.tc_p;

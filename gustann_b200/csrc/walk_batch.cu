@@ -314,12 +314,13 @@ __global__ void __launch_bounds__(W * 32, 24 / W) batch_search_kernel(BatchParam
   const PqView pv{p.ix.pivots_t, p.ix.centroid, p.ix.chunk_off, M, dim, p.fma};
   uint32_t* const list_id = s.l_id;
   float* const list_d = s.l_d;
+  const int nq = p.nq_dev ? min(p.nq, *p.nq_dev) : p.nq;
 
   for (;;) {
     if (tid == 0) s.ctrl[0] = atomicAdd(p.next_query, 1);
     __syncthreads();
     const int qid = s.ctrl[0];
-    if (qid >= p.nq) break;
+    if (qid >= nq) break;
     const int L = p.L_per_q ? min(max(__ldg(p.L_per_q + qid), 1), p.L_max) : p.L_max;
     const int k = p.k_per_q ? min(max(__ldg(p.k_per_q + qid), 1), p.k_max) : p.k_max;
     for (int i = tid; i < dim; i += NT) s.q[i] = __ldg(p.queries + (size_t)qid * dim + i);

@@ -192,6 +192,29 @@ int gann_search_batch_noalloc(gann_t* h, const float* d_queries, int nq, int top
                               const gann_batch_opts_t* opts, int32_t* d_nns, float* d_distances,
                               int32_t* d_found_cnt, void* stream);
 
+/*
+ * Batched search captured once as a CUDA graph (counter reset, tensor-core
+ * table build, persistent walk) and replayed by gann_batch_graph_launch. The
+ * device buffers given here are baked into the graph: d_queries (max_nq x dim),
+ * optional per-query d_topk / d_ef_search (NULL = topk_max / ef_max for all),
+ * the outputs as in gann_search_batch_device, and d_nq, a device int holding
+ * the number of queries (rows from 0) each launch processes, read by the
+ * kernels at run time and clamped to max_nq. Write the queries and the count,
+ * launch, read the results. Options (precision, beam width, visited cache) and
+ * the handle's tuned defaults are fixed at capture. Launches of one graph run
+ * one after another; graphs of one handle may run concurrently. The reference
+ * launches its kernels once per call (src/pure_mem.cu:101-184); no counterpart.
+ */
+typedef struct gann_batch_graph gann_batch_graph_t;
+int gann_batch_graph_create(gann_t* h, int max_nq, int topk_max, int ef_max, const gann_batch_opts_t* opts,
+                            const float* d_queries, const int32_t* d_topk, const int32_t* d_ef_search,
+                            const int32_t* d_nq, int32_t* d_nns, float* d_distances, int32_t* d_found_cnt,
+                            gann_batch_graph_t** out);
+/* Enqueue one replay on `stream` (a cudaStream_t; NULL = the graph's own stream). */
+int gann_batch_graph_launch(gann_batch_graph_t* g, void* stream);
+/* Wait for the graph's own stream and release the graph and its scratch. NULL is accepted. */
+int gann_batch_graph_destroy(gann_batch_graph_t* g);
+
 /* PQ distance tables of nq host queries (tables: nq x M x 256 FP32, host),
  * built as the chosen precision builds them: FP32 exactly as the plain form
  * (PQSearchData::init_query, src/impl/pq.cuh:8-59); the BF16 forms widened

@@ -175,3 +175,41 @@ def test_autotune_sets_the_defaults(scale):
     explicit = g.search_batch(q, 10, 128, precision=gb.PREC_BF16, beam_width=W, hash_bits=hb)
     np.testing.assert_array_equal(tuned[0], explicit[0])
     np.testing.assert_array_equal(tuned[1].view(np.uint32), explicit[1].view(np.uint32))
+
+
+@pytest.mark.gpu
+def test_graph_replays_match_batch(scale):
+    """gann_batch_graph_*: one capture, replayed with run-time counts 300, 0,
+    500 and 37 read from device memory; each replay's rows equal
+    gann_search_batch on the same queries, rows past the count stay untouched."""
+    import torch
+
+    g, q, gt = scale
+    q = np.ascontiguousarray(q[:500])
+    L, k = synth.draws(len(q), [32, 64, 128, 256], [1, 10, 100])
+    L, k = L.astype(np.int32), k.astype(np.int32)
+    for prec in (gb.PREC_BF16, gb.PREC_FP32):
+        ids, dis, fnd, _ = g.search_batch(q, k, L, precision=prec, beam_width=4, hash_bits=11)
+        dq, dk, dl = (torch.from_numpy(x).cuda() for x in (q, k, L))
+        dn = torch.zeros(1, dtype=torch.int32, device="cuda")
+        nns = torch.empty((500, 100), dtype=torch.int32, device="cuda")
+        dd = torch.empty((500, 100), dtype=torch.float32, device="cuda")
+        df = torch.empty(500, dtype=torch.int32, device="cuda")
+        bg = gb.BatchGraph(g, 500, 100, 256, dq.data_ptr(), dn.data_ptr(), nns.data_ptr(), dd.data_ptr(),
+                           df.data_ptr(), d_topk=dk.data_ptr(), d_ef=dl.data_ptr(), precision=prec, beam_width=4,
+                           hash_bits=11)
+        for n in (300, 0, 500, 37):
+            nns.fill_(-7)
+            df.fill_(-7)
+            dn.fill_(n)
+            torch.cuda.synchronize()
+            bg.launch()
+            torch.cuda.synchronize()
+            gi, gd, gf = nns.cpu().numpy(), dd.cpu().numpy(), df.cpu().numpy()
+            np.testing.assert_array_equal(gf[:n], fnd[:n])
+            for i in range(n):
+                np.testing.assert_array_equal(gi[i, :k[i]], ids[i, :k[i]])
+                np.testing.assert_array_equal(gd[i, :k[i]].view(np.uint32), dis[i, :k[i]].view(np.uint32))
+            assert (gi[n:] == -7).all() and (gf[n:] == -7).all()
+        bg.destroy()
+    g.check()
