@@ -176,3 +176,15 @@ def test_pq_legacy_and_new_tables_agree(golden, tmp_path, oracle_mod):
     o2 = oracle_mod.Oracle(str(d / "index_disk.index"), str(d / "index_pq"), str(d / "nav"), 0)
     for x, t in zip(q, t_new):
         np.testing.assert_array_equal(o2.pq_table(x)[0], t)
+
+
+def test_record_division_is_exact(tmp_path):
+    """gann::FastDiv (multiply-shift division by nodes-per-page, used to address
+    records in the batched walk) equals integer division for ids below 2^31."""
+    import subprocess
+
+    exe = tmp_path / "fastdiv_check"
+    subprocess.run(["g++", "-std=c++17", "-O2", "-I", "/usr/local/cuda/include", "-I", str(ROOT / "include"),
+                    str(ROOT / "tests" / "fastdiv_check.cpp"), "-o", str(exe)], check=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and r.stdout.startswith("ok"), r.stdout + r.stderr
