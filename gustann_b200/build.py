@@ -54,6 +54,22 @@ def _stale(target: Path, deps: list[Path]) -> bool:
     return any(d.stat().st_mtime > t for d in deps)
 
 
+CLI = PKG / "search_mem"
+
+
+def build_cli(verbose: bool = False, force: bool = False) -> Path:
+    """Compile the search_mem driver (cli/search_mem.cpp) against libgann.so."""
+    src = PKG / "cli" / "search_mem.cpp"
+    deps = [src, LIB, ROOT / "include" / "gann.h", ROOT / "include" / "gustann.hpp"]
+    if force or _stale(CLI, deps):
+        cmd = ["g++", "-std=c++17", "-O2", "-I", str(ROOT / "include"), str(src), "-o", str(CLI), "-L", str(PKG),
+               "-lgann", "-Wl,-rpath,$ORIGIN"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    return CLI
+
+
 def build_lib(verbose: bool = False, force: bool = False) -> Path:
     """Compile csrc/ into gustann_b200/libgann.so (incremental)."""
     nvcc = _nvcc()
@@ -97,5 +113,6 @@ def build_oracle(verbose: bool = False) -> None:
 
 if __name__ == "__main__":
     build_lib(verbose="-v" in sys.argv, force="-f" in sys.argv)
+    build_cli(verbose="-v" in sys.argv, force="-f" in sys.argv)
     build_oracle(verbose="-v" in sys.argv)
     print(LIB)

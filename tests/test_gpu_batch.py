@@ -62,6 +62,33 @@ def test_table_precision_against_fp64(golden, oracle_mod, name):
     assert err[gb.PREC_BF16] <= 2.0 ** -5, err
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["u8_nav", "f32_nav"])
+def test_rerank_distance_against_fp64(golden, name):
+    """Exact-rerank distances of the returned ids against FP64: the batched
+    form's int32 path is exact for uint8 vectors with integral queries; FP32
+    reranks (batched on float data, and the plain form) stay within
+    dim * 2^-24 of the FP64 distance, relative."""
+    from gustann_b200.indexing import formats
+
+    meta = golden[name]
+    g = open_meta(meta)
+    q = meta["queries"]
+    vecs = formats.read_disk_index(meta["index_file"], np.uint8 if meta["dtype"] == 0 else np.float32).data
+    dim = q.shape[1]
+    forms = {"batched": g.search_batch(q, 10, 40, precision=gb.PREC_BF16)[:3], "plain": g.query(q, 10, 40)[:3]}
+    for form, (ids, dis, fnd) in forms.items():
+        worst = 0.0
+        for i in range(len(q)):
+            v = vecs[ids[i, :fnd[i]]].astype(np.float64)
+            d64 = ((v - q[i].astype(np.float64)) ** 2).sum(1)
+            rel = np.abs(dis[i, :fnd[i]].astype(np.float64) - d64) / np.maximum(d64, 1e-30)
+            worst = max(worst, float(rel.max()) if len(rel) else 0.0)
+        if form == "batched" and meta["dtype"] == 0:
+            assert worst == 0.0, (form, worst)
+        assert worst <= dim * 2.0 ** -24, (form, worst)
+
+
 @pytest.fixture(scope="module")
 def scale(tmp_path_factory):
     d = tmp_path_factory.mktemp("bscale")
