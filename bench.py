@@ -460,6 +460,25 @@ def _run_ours(args, rank, world, local):
                          use_gpu_mem=False)
         runners["host_plain"] = PlainRunner(gh, q, k)
         runners["host_batched_bf16"] = BatchRunner(gh, q, k, gb.PREC_BF16, args.beam, "host_batched_bf16")
+    gc, cache_info = None, None
+    if "host_batched_bf16_cached" in args.forms.split(","):
+        # host-memory records plus an HBM cache of the hottest ones, chosen by a
+        # sample batch of base vectors (not the timed queries)
+        from gustann_b200.indexing import formats
+
+        gc = gb.GustANN(dtype)
+        gc.init_pure_mem(gb.GustANNConfig(meta["index_file"], meta["pq_prefix"], meta["nav_dir"] or ""),
+                         use_gpu_mem=False)
+        di = formats.read_disk_index(meta["index_file"], np.uint8 if meta["kind"] == "u8" else np.float32)
+        pick = np.random.default_rng(11).choice(di.n, size=min(di.n, 2000), replace=False)
+        sample = torch.from_numpy(np.ascontiguousarray(di.data[pick], dtype=np.float32)).cuda()
+        del di
+        budget = int(gc.info()["host_bytes"] * args.host_cache)
+        n_cached = gc.cache_hot_records(sample.data_ptr(), sample.shape[0], args.tune_L, budget)
+        cache_info = {"fraction_of_page_bytes": args.host_cache, "budget_bytes": budget, "records": n_cached,
+                      "sample": f"{sample.shape[0]} base vectors at L {args.tune_L}"}
+        runners["host_batched_bf16_cached"] = BatchRunner(gc, q, k, gb.PREC_BF16, args.beam,
+                                                          "host_batched_bf16_cached")
     forms = [f for f in args.forms.split(",") if f in runners]
     tuned = None
     if args.beam == 0 and any(f != "plain" for f in forms):  # autotuner: beam width and visited cache
@@ -468,7 +487,7 @@ def _run_ours(args, rank, world, local):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     res = {}
     for f in forms:  # a host-paged form runs at the L of its HBM twin (same results, same recall)
-        twin = res.get(f[5:]) if f.startswith("host_") else None
+        twin = res.get(f[5:].replace("_cached", "")) if f.startswith("host_") else None
         res[f] = measure_form(runners[f], args, gt, world, flush, local, twin["L"] if twin else None)
     ok = [f for f in forms if res[f]["recall"] >= args.recall and not f.startswith("host_")]
     head = args.headline if args.headline in ok else (max(ok, key=lambda f: res[f]["qps"]) if ok else forms[0])
@@ -509,6 +528,7 @@ def _run_ours(args, rank, world, local):
                       "hops_per_query": v["hops_per_query"], "gathered_bytes_per_query": v["bytes_per_step"] / nq}
                   for f, v in res.items()},
         "build_s": meta.get("build_s"),
+        "host_record_cache": cache_info,
     }
     if "plain" in res and head != "plain":
         out["speedup_vs_plain"] = r["qps"] / res["plain"]["qps"]
@@ -521,6 +541,8 @@ def _run_ours(args, rank, world, local):
     g.close()
     if gh is not None:
         gh.close()
+    if gc is not None:
+        gc.close()
     barrier(world)
     if world > 1:
         import torch.distributed as dist
@@ -628,7 +650,10 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true")
-    ap.add_argument("--forms", default="plain,batched_bf16,batched_bf16x3,batched_fp32,host_plain,host_batched_bf16")
+    ap.add_argument("--forms", default="plain,batched_bf16,batched_bf16x3,batched_fp32,host_plain,host_batched_bf16,"
+                                       "host_batched_bf16_cached")
+    ap.add_argument("--host-cache", type=float, default=0.1,
+                    help="HBM record cache of the host_batched_bf16_cached form, as a fraction of the page bytes")
     ap.add_argument("--headline", default="batched_bf16")
     ap.add_argument("--beam", type=int, default=0, help="0 = autotune (gann_autotune)")
     ap.add_argument("--tune-L", type=int, default=384)

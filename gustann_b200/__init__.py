@@ -108,6 +108,7 @@ _SIGNATURES = {
     "gann_batch_graph_create": (_I, [_P, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P, ctypes.POINTER(_P)]),
     "gann_batch_graph_launch": (_I, [_P, _P]),
     "gann_batch_graph_destroy": (_I, [_P]),
+    "gann_cache_hot_records": (_I, [_P, _P, _I, _I, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]),
     "gann_pq_tables": (_I, [_P, _P, _I, _I, _P]),
     "gann_autotune": (_I, [_P, _P, _I, _I, _I, _I, _P, ctypes.POINTER(ctypes.c_double)]),
     "gann_server_start": (_I, [_P, ctypes.POINTER(ServerOpts), ctypes.POINTER(_P)]),
@@ -300,6 +301,14 @@ class GustANN:
         out = np.zeros((q.shape[0], M, 256), np.float32)
         _check(lib().gann_pq_tables(self.handle, _ptr(q), q.shape[0], int(precision), _ptr(out)))
         return out
+
+    def cache_hot_records(self, d_q: int, nq: int, ef_search: int, max_bytes: int) -> int:
+        """gann_cache_hot_records (host-memory records only): copy the records a
+        sample batch of nq device queries expands most into HBM, up to max_bytes.
+        Returns the number of records cached."""
+        n = ctypes.c_int64(0)
+        _check(lib().gann_cache_hot_records(self.handle, d_q, nq, ef_search, int(max_bytes), ctypes.byref(n)))
+        return n.value
 
     def check(self, stream: int | None = None) -> None:
         _check(lib().gann_check(self.handle, _stream(stream)))

@@ -3,6 +3,7 @@
 // gann_open   ~ GustANN::GustANN + GustANN::init_pure_mem(cfg, true)  (src/ssd_search.cu:55-112,
 //               src/pure_mem.cu:27-69)
 // gann_search ~ GustANN::search -> PureMemExecutor::search            (src/pure_mem.cu:71-199)
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -145,6 +146,9 @@ void free_all(gann_index* h) {
   if (h->host_pages) cudaFreeHost(h->host_pages);
   h->host_pages = nullptr;
   h->host_bytes = 0;
+  h->dx.rec_remap = nullptr;  // both freed with the allocations above
+  h->dx.rec_cache = nullptr;
+  h->dx.rec_stride = 0;
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -431,7 +435,8 @@ int batch_hash_bits(int ef_max) {
 int enqueue_batch(gann_t* h, const float* d_q, int nq, const int32_t* d_k, const int32_t* d_l, int k_max,
                   int l_max, const gann_batch_opts_t* opts, int32_t* d_nns, float* d_dists, int32_t* d_found,
                   int32_t* d_hops, int64_t* d_bytes, cudaStream_t s, int* counter = nullptr,
-                  __nv_bfloat16* tables = nullptr, const int* nq_dev = nullptr) {
+                  __nv_bfloat16* tables = nullptr, const int* nq_dev = nullptr,
+                  int32_t* visit_count = nullptr) {
   gann_batch_opts_t o{};
   if (opts) o = *opts;
   const int prec = opts ? o.precision : GANN_PREC_BF16;
@@ -462,6 +467,7 @@ int enqueue_batch(gann_t* h, const float* d_q, int nq, const int32_t* d_k, const
   p.queries = d_q;
   p.nq = nq;
   p.nq_dev = nq_dev;
+  p.visit_count = visit_count;
   p.L_per_q = d_l;
   p.k_per_q = d_k;
   p.L_max = l_max;
@@ -736,3 +742,93 @@ int gann_internal_enqueue_batch_dev(gann_t* h, const float* d_q, int nq, const i
                        counter, tables, nq_dev);
 }
 
+extern "C" int gann_cache_hot_records(gann_t* h, const float* d_queries, int nq, int ef_search, int64_t max_bytes,
+                           int64_t* cached_records) {
+  if (!h) return set_error(GANN_EINVAL, "null handle");
+  if (cached_records) *cached_records = 0;
+  if (!h->host_pages) return set_error(GANN_EINVAL, "the records are already in HBM (open with GANN_OPEN_HOST_PAGES)");
+  if (nq < 1 || !d_queries) return set_error(GANN_EINVAL, "a sample of at least one device query is needed");
+  if (ef_search < 1 || ef_search > 4096) return set_error(GANN_EINVAL, "ef_search must be in 1..4096");
+  if (max_bytes < 0) return set_error(GANN_EINVAL, "max_bytes must be >= 0");
+  std::lock_guard<std::mutex> lk(h->mu);
+  const gann::HostIndex& hx = h->hx;
+  const int64_t stride = (hx.node_len + 15) / 16 * 16;
+  const int64_t slots = std::min<int64_t>(hx.n, std::min<int64_t>(max_bytes / stride, INT32_MAX));
+  int32_t* d_count = nullptr;
+  int32_t* d_nns = nullptr;
+  float* d_dists = nullptr;
+  int32_t* d_found = nullptr;
+  auto release = [&]() {
+    for (void* p : {(void*)d_count, (void*)d_nns, (void*)d_dists, (void*)d_found})
+      if (p) cudaFree(p);
+  };
+  auto fail = [&](int code, const std::string& m) {
+    release();
+    return set_error(code, m);
+  };
+  // 1. expansion counts of a sample batch (the batched walk, BF16 tensor-core
+  //    tables where available, counting each expanded node).
+  cudaError_t e = cudaMalloc(&d_count, sizeof(int32_t) * hx.n);
+  if (e == cudaSuccess) e = cudaMalloc(&d_nns, sizeof(int32_t) * nq);
+  if (e == cudaSuccess) e = cudaMalloc(&d_dists, sizeof(float) * nq);
+  if (e == cudaSuccess) e = cudaMalloc(&d_found, sizeof(int32_t) * nq);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_count, 0, sizeof(int32_t) * hx.n, h->stream);
+  if (e != cudaSuccess) return fail(GANN_ENOMEM, "record cache: sample buffers");
+  gann_batch_opts_t o{};
+  o.precision = h->dx.tc_bpanel_hi ? GANN_PREC_BF16 : GANN_PREC_BF16_CC;
+  const int rc = enqueue_batch(h, d_queries, nq, nullptr, nullptr, 1, ef_search, &o, d_nns, d_dists, d_found,
+                               nullptr, nullptr, h->stream, nullptr, nullptr, nullptr, d_count);
+  if (rc != GANN_OK) return fail(rc, g_last_error);
+  std::vector<int32_t> count((size_t)hx.n);
+  e = cudaMemcpyAsync(count.data(), d_count, sizeof(int32_t) * hx.n, cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return fail(GANN_ECUDA, std::string("record cache: sample run: ") + cudaGetErrorString(e));
+  release();
+  // 2. the hottest records, most expansions first (ties by id), up to the budget
+  std::vector<int32_t> ids;
+  for (int64_t u = 0; u < hx.n; u++)
+    if (count[u] > 0) ids.push_back((int32_t)u);
+  auto hotter = [&](int32_t a, int32_t b) { return count[a] > count[b] || (count[a] == count[b] && a < b); };
+  if ((int64_t)ids.size() > slots) {
+    std::nth_element(ids.begin(), ids.begin() + slots, ids.end(), hotter);
+    ids.resize(slots);
+  }
+  std::sort(ids.begin(), ids.end(), hotter);
+  // 3. copy them (verbatim, from the pinned page body) and the id -> slot map to HBM
+  std::vector<int32_t> remap((size_t)hx.n, -1);
+  std::vector<uint8_t> cache((size_t)ids.size() * stride, 0);
+  for (size_t i = 0; i < ids.size(); i++) {
+    const int64_t u = ids[i];
+    std::memcpy(&cache[i * stride], h->host_pages + (u / hx.npp) * gann::kPageSize + (u % hx.npp) * hx.node_len,
+                (size_t)hx.node_len);
+    remap[u] = (int32_t)i;
+  }
+  try {
+    // drop an earlier cache first (its two allocations are the last ones made)
+    if (h->dx.rec_remap) {
+      for (const void* p : {(const void*)h->dx.rec_remap, (const void*)h->dx.rec_cache}) {
+        auto it = std::find(h->allocations.begin(), h->allocations.end(), p);
+        if (it != h->allocations.end()) {
+          cudaFree(*it);
+          h->allocations.erase(it);
+        }
+      }
+      h->device_bytes -= (int64_t)sizeof(int32_t) * hx.n + h->rec_cache_bytes;
+      h->dx.rec_remap = nullptr;
+      h->dx.rec_cache = nullptr;
+      h->rec_cache_bytes = 0;
+    }
+    if (ids.empty()) return GANN_OK;
+    uint8_t* d_cache = upload(h, cache);
+    int32_t* d_remap = upload(h, remap);
+    h->dx.rec_cache = d_cache;
+    h->dx.rec_remap = d_remap;
+    h->dx.rec_stride = stride;
+    h->rec_cache_bytes = (int64_t)cache.size();
+  } catch (const CudaFail& ce) {
+    return set_error(ce.e == cudaErrorMemoryAllocation ? GANN_ENOMEM : GANN_ECUDA,
+                     std::string("record cache: ") + ce.what + ": " + cudaGetErrorString(ce.e));
+  }
+  if (cached_records) *cached_records = (int64_t)ids.size();
+  return GANN_OK;
+}

@@ -91,7 +91,24 @@ struct DeviceIndex {
   const float* tc_pnorm = nullptr;        // M x 256
   int tc_p = 0, tc_groups = 0;            // padded chunk width, chunk groups per K=16 slice
   unsigned int* err = nullptr;            // kernel error word
+  // HBM copies of hot records when the pages sit in host memory
+  // (gann_cache_hot_records): rec_remap[u] = cache slot of node u, or -1.
+  const int32_t* rec_remap = nullptr;     // n, or null (no cache)
+  const uint8_t* rec_cache = nullptr;     // slots x rec_stride, records copied verbatim
+  int64_t rec_stride = 0;
 };
+
+// Address of node u's record: its HBM copy when it is cached, else its page slot.
+#ifdef __CUDACC__
+__device__ __forceinline__ const uint8_t* record_at(const DeviceIndex& ix, int64_t page, int64_t slot_off,
+                                                    int64_t u) {
+  if (ix.rec_remap) {
+    const int32_t c = __ldg(ix.rec_remap + u);
+    if (c >= 0) return ix.rec_cache + (int64_t)c * ix.rec_stride;
+  }
+  return ix.pages + page * kPageSize + slot_off;
+}
+#endif
 
 // Launch parameters of the plain search kernel (walk_plain.cu).
 struct PlainParams {
@@ -125,6 +142,7 @@ struct BatchParams {
   int L_max, k_max;
   int hash_bits;                  // visited cache: 1 << hash_bits slots
   FastDiv npp_div;                // division by nodes per page
+  int32_t* visit_count;           // or null: per-node expansion counts (gann_cache_hot_records)
   const __nv_bfloat16* tables;    // nq x M x 256 BF16 tables built for the batch, or null
   int fma;
   int32_t* nns;                   // nq x k_max
@@ -184,6 +202,7 @@ struct gann_index {
   int64_t device_bytes = 0;
   uint8_t* host_pages = nullptr;   // pinned, mapped page body (GANN_OPEN_HOST_PAGES)
   int64_t host_bytes = 0;
+  int64_t rec_cache_bytes = 0;     // HBM record cache (gann_cache_hot_records)
   int* d_counter = nullptr;       // work counter scratch (plain kernel)
   unsigned int* d_err = nullptr;   // kernel error word
   // per-call device buffers, grown on demand

@@ -287,7 +287,7 @@ struct Record {
     uok = id >= 0 && id < p.n;
     const uint32_t uu = uok ? (uint32_t)id : 0u;
     const uint32_t pg = p.npp_div.div(uu);
-    node = p.ix.pages + (int64_t)pg * kPageSize + (int64_t)(uu - pg * (uint32_t)p.npp) * p.node_len;
+    node = record_at(p.ix, pg, (int64_t)(uu - pg * (uint32_t)p.npp) * p.node_len, uu);
     meta = reinterpret_cast<const int32_t*>(node + p.data_len);
     deg = __ldg(meta);
 #pragma unroll
@@ -476,6 +476,7 @@ __global__ void __launch_bounds__(W * 32, 24 / W) batch_search_kernel(BatchParam
         if (lane == 0) {
           s.sel_d[warp] = ed;
           s.sel_id[warp] = (int32_t)rec.u;
+          if (p.visit_count && ok) atomicAdd(p.visit_count + rec.u, 1);
         }
         gathered += ok ? 4 + 4 * deg + p.data_len + (int64_t)nnew * M : 0;
       }

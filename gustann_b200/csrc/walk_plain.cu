@@ -104,7 +104,7 @@ __device__ void search_query(const PlainParams& p, const WarpSmem& s, int qid, i
       if (lane == 0) atomicOr(p.err, kErrHopCap);
       break;
     }
-    const uint8_t* node = p.ix.pages + (u / p.npp) * kPageSize + (u % p.npp) * p.node_len;
+    const uint8_t* node = record_at(p.ix, u / p.npp, (u % p.npp) * p.node_len, u);
     const int32_t* meta = reinterpret_cast<const int32_t*>(node + p.data_len);
     const int deg = __ldg(meta);
     if (deg < 0 || deg > max_m) {

@@ -99,6 +99,19 @@ typedef struct {
 int gann_open(const char* index_file, const char* pq_prefix, const char* nav_dir, int dtype,
               int flags, gann_t** out);
 
+/*
+ * For a handle opened with GANN_OPEN_HOST_PAGES: copy the records most often
+ * expanded by a sample batch (nq device queries searched at ef_search) into
+ * HBM, up to max_bytes (records padded to 16 B), and read those from HBM from
+ * then on; the others stay in host memory. Results do not change (the same
+ * bytes are read). A later call replaces the cache; max_bytes 0 drops it.
+ * *cached_records (may be NULL) receives the number cached. The reference's
+ * host-memory mode reads every record over the bus (src/pure_mem.cu:51-66,
+ * src/impl/pure_mem.cuh:50-241); no counterpart.
+ */
+int gann_cache_hot_records(gann_t* h, const float* d_queries, int nq, int ef_search, int64_t max_bytes,
+                           int64_t* cached_records);
+
 /* Release the handle and its device memory. Replaces gustann::GustANN::~GustANN,
  * src/ssd_search.cu:29-53. NULL is accepted. */
 int gann_close(gann_t* h);

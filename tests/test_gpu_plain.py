@@ -220,3 +220,37 @@ def test_host_pages_match_hbm_at_scale(scale_index):
         assert_same(b[0], b[1], b[2], a[0], a[1], a[2], f"host vs hbm batched precision={prec}")
     hbm.close()
     host.close()
+
+
+@pytest.mark.gpu
+def test_record_cache_keeps_results(scale_index):
+    """gann_cache_hot_records on a host-memory handle: the hottest records of a
+    sample batch move to HBM and every search returns the same ids, distances
+    and counts; a smaller cache replaces it, a zero budget drops it; an HBM
+    handle refuses it."""
+    import torch
+
+    f, q, gt = scale_index
+    cfg = gb.GustANNConfig(f.index_file, f.pq_prefix, f.nav_dir)
+    host = gb.GustANN(gb.DataType.UINT8)
+    host.init_pure_mem(cfg, use_gpu_mem=False)
+    before = (host.query(q, 10, 64), host.search_batch(q, 10, 128))
+    dq = torch.from_numpy(np.ascontiguousarray(q[:500])).cuda()
+    inf = host.info()
+    stride = (inf["node_len"] + 15) // 16 * 16
+    budget = inf["num_points"] * stride // 5
+    dev0 = inf["device_bytes"]
+    for b in (budget, budget // 4, 0):
+        n = host.cache_hot_records(dq.data_ptr(), 500, 128, b)
+        assert 0 <= n <= b // stride and (n > 0) == (b > 0)
+        assert host.info()["device_bytes"] == dev0 + (n * stride + 4 * inf["num_points"] if n else 0)
+        after = (host.query(q, 10, 64), host.search_batch(q, 10, 128))
+        for (ai, ad, af, _), (bi, bd, bf, _) in zip(before, after):
+            assert_same(bi, bd, bf, ai, ad, af, f"record cache {b} bytes")
+    host.close()
+    hbm = gb.GustANN(gb.DataType.UINT8)
+    hbm.init_pure_mem(cfg)
+    with pytest.raises(gb.GustANNError) as e:
+        hbm.cache_hot_records(dq.data_ptr(), 500, 128, budget)
+    assert e.value.code == gb.GANN_EINVAL
+    hbm.close()
