@@ -221,12 +221,38 @@ __device__ __forceinline__ void topk_push_many(float* td, int32_t* ti, int& size
 }
 
 // Exact squared L2 of the node (its first kVecRegs*32 elements preloaded in
-// vx, lane-strided). uint8 vectors with an integral query are summed in int32
-// (exact); otherwise FP32 with the reference's reduction (util.cuh:26-46).
-template <class T>
-__device__ __forceinline__ float exact_dist(const float* q, const T* v, const float (&vx)[kVecRegs], int dim,
-                                            int lane, bool int_query, int fma) {
-  if (sizeof(T) == 1 && int_query) {
+// vx, lane-strided; or, PK, a uint8 vector of dim <= 128 held as one 32-bit
+// word per lane, bytes 4 lane .. 4 lane + 3). uint8 vectors with an integral
+// query are summed in int32 (exact); otherwise FP32 with the reference's
+// reduction (util.cuh:26-46), the PK form first moving each lane's strided
+// elements into place with shuffles so the sum is the same.
+template <class T, bool PK>
+__device__ __forceinline__ float exact_dist(const float* q, const T* v, const float (&vx_in)[kVecRegs], uint32_t vw,
+                                            int dim, int lane, bool int_query, int fma) {
+  if (PK && int_query) {
+    int acc = 0;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const int i = 4 * lane + j;
+      if (i < dim) {
+        const int d = (int)q[i] - (int)((vw >> (8 * j)) & 0xffu);
+        acc += d * d;
+      }
+    }
+    acc = __reduce_add_sync(kFull, acc);
+    return (float)acc;
+  }
+  float vx[kVecRegs];
+#pragma unroll
+  for (int r = 0; r < kVecRegs; r++) {
+    if (PK) {
+      const uint32_t w = __shfl_sync(kFull, vw, (lane + 32 * r) >> 2);
+      vx[r] = (float)((w >> (8 * (lane & 3))) & 0xffu);
+    } else {
+      vx[r] = vx_in[r];
+    }
+  }
+  if (!PK && sizeof(T) == 1 && int_query) {
     int acc = 0;
 #pragma unroll
     for (int r = 0; r < kVecRegs; r++) {
@@ -273,7 +299,7 @@ constexpr int kStage = 4;  // list entries per thread staged in registers by the
 
 // The node's record as one warp holds it: degree, the first kEdgeRegs * 32
 // neighbour slots and kVecRegs * 32 vector elements, loaded in one round trip.
-template <class T>
+template <class T, bool PK>
 struct Record {
   int64_t u = -1;
   bool uok = false;
@@ -281,7 +307,8 @@ struct Record {
   const int32_t* meta = nullptr;
   int deg = 0;
   int ev[kEdgeRegs];
-  float vx[kVecRegs];
+  float vx[kVecRegs];  // lane-strided elements (not PK)
+  uint32_t vw = 0;     // PK: bytes 4 lane .. 4 lane + 3 of a uint8 vector, one 128-byte load per warp
   __device__ __forceinline__ void load(const BatchParams& p, int64_t id, int lane) {
     u = id;
     uok = id >= 0 && id < p.n;
@@ -292,13 +319,17 @@ struct Record {
     deg = __ldg(meta);
 #pragma unroll
     for (int r = 0; r < kEdgeRegs; r++) ev[r] = lane + 32 * r < p.max_m ? __ldg(meta + 1 + lane + 32 * r) : -1;
+    if (PK) {
+      vw = 4 * lane < p.dim ? __ldg(reinterpret_cast<const uint32_t*>(node) + lane) : 0u;
+    } else {
 #pragma unroll
-    for (int r = 0; r < kVecRegs; r++)
-      vx[r] = lane + 32 * r < p.dim ? load_elem<T>(reinterpret_cast<const T*>(node), lane + 32 * r) : 0.0f;
+      for (int r = 0; r < kVecRegs; r++)
+        vx[r] = lane + 32 * r < p.dim ? load_elem<T>(reinterpret_cast<const T*>(node), lane + 32 * r) : 0.0f;
+    }
   }
 };
 
-template <class T, class TabT, int W>
+template <class T, class TabT, int W, bool PK>
 __global__ void __launch_bounds__(W * 32, 24 / W) batch_search_kernel(BatchParams p) {
   constexpr int NT = W * 32;
   constexpr int TKW = W - 1;  // warp that marks the picks and keeps the top-k
@@ -378,7 +409,7 @@ __global__ void __launch_bounds__(W * 32, 24 / W) batch_search_kernel(BatchParam
     int pick_pos[W];
 #pragma unroll
     for (int w = 0; w < W; w++) pick_pos[w] = w == 0 && u0 >= 0 ? 0 : -1;
-    Record<T> rec;
+    Record<T, PK> rec;
     if (warp == 0 && u0 >= 0) rec.load(p, u0, lane);
 
     for (;;) {
@@ -467,7 +498,9 @@ __global__ void __launch_bounds__(W * 32, 24 / W) batch_search_kernel(BatchParam
           cw1 = __ldg(c4 + 1);
         }
         float ed = inf_f();
-        if (ok) ed = exact_dist<T>(s.q, reinterpret_cast<const T*>(rec.node), rec.vx, dim, lane, int_query, p.fma);
+        if (ok)
+          ed = exact_dist<T, PK>(s.q, reinterpret_cast<const T*>(rec.node), rec.vx, rec.vw, dim, lane, int_query,
+                                 p.fma);
         if (has) keep(v0, m32 ? adc32_words(table, cw0, cw1) : adc_split4(table, p.ix.codes + (size_t)v0 * M, M));
         for (int i = lane + 32; i < nnew; i += 32) {
           const uint32_t v = wnew[i];
@@ -685,12 +718,12 @@ __global__ void __launch_bounds__(W * 32, 24 / W) batch_search_kernel(BatchParam
   }
 }
 
-template <class T, class TabT, int W>
-cudaError_t launch_w(const BatchParams& p, int num_sms, cudaStream_t stream) {
+template <class T, class TabT, int W, bool PK>
+cudaError_t launch_wp(const BatchParams& p, int num_sms, cudaStream_t stream) {
   const BatchPlan pl(p.M, (int)sizeof(TabT), 1 << p.hash_bits, p.L_max, p.max_m, W, p.k_max, p.dim);
   const size_t smem = pl.total;
   if (smem > 227 * 1024) return cudaErrorInvalidConfiguration;
-  auto kern = batch_search_kernel<T, TabT, W>;
+  auto kern = batch_search_kernel<T, TabT, W, PK>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
@@ -701,6 +734,16 @@ cudaError_t launch_w(const BatchParams& p, int num_sms, cudaStream_t stream) {
   if (grid > p.nq) grid = p.nq;
   kern<<<grid, W * 32, smem, stream>>>(p);
   return cudaGetLastError();
+}
+
+// uint8 vectors of dim <= 128, a multiple of 4, in 4-byte aligned records
+// (every record start is then 4-byte aligned) load as one word per lane.
+template <class T, class TabT, int W>
+cudaError_t launch_w(const BatchParams& p, int num_sms, cudaStream_t stream) {
+  const bool pk = sizeof(T) == 1 && p.dim % 4 == 0 && p.dim <= 128 && p.node_len % 4 == 0 &&
+                  (p.ix.rec_stride == 0 || p.ix.rec_stride % 4 == 0);
+  if (pk) return launch_wp<T, TabT, W, true>(p, num_sms, stream);
+  return launch_wp<T, TabT, W, false>(p, num_sms, stream);
 }
 
 template <class T, class TabT>
