@@ -7,10 +7,13 @@
 // built on the tensor cores for the whole batch); then a beam walk that expands
 // up to W candidates per step, one per warp (src/impl/pure_mem.cuh:243-432
 // expands one):
+//   * the picks of a step are the first W unexpanded list entries; each step
+//     works them out for the next one from its sorted survivors before it
+//     rewrites the list, so every warp's next record loads during the merge;
 //   * a direct-mapped cache of the ids already scored for this query (the
 //     visited filter) skips their code gather and ADC. A hit is always a node
-//     the list has already considered (the entry node is listed as expanded),
-//     and a node the list has considered is rejected when it is scored again:
+//     the list has already considered (the entry node is listed too), and a
+//     node the list has considered is rejected when it is scored again:
 //     it is either still in the list (same key) or at or above the list's last
 //     key, which only decreases. So the cache's contents, which depend on the
 //     order of the warps' atomicExch, change the work done but never the result;
