@@ -420,6 +420,9 @@ def measure_form(runner, args, gt, world, flush, local, fixed_L=None):
     L, rec = calibrate(runner, gt, args.k, args.recall, fixed_L or args.L or None)
     runner.run(L, counters=True)
     torch.cuda.synchronize()
+    from gustann_b200.indexing.groundtruth import recall_unique
+
+    rec_u = recall_unique(runner.ids.cpu().numpy(), gt, args.k)
     hops = runner.hops.cpu().numpy()
     step_bytes = int(runner.bytes.sum().item())
     clocks = ClockSampler(local)
@@ -427,7 +430,7 @@ def measure_form(runner, args, gt, world, flush, local, fixed_L=None):
     times_ms = time_steps(runner, L, args.steps, args.warmup, world, flush)
     clk = clocks.stop()
     total_ms = max_over_ranks(float(sum(times_ms)), world, device="cuda")
-    return {"L": L, "recall": rec, "total_ms": total_ms, "avg_ms": float(np.mean(times_ms)),
+    return {"L": L, "recall": rec, "recall_unique": rec_u, "total_ms": total_ms, "avg_ms": float(np.mean(times_ms)),
             "qps": world * runner.nq * args.steps / (total_ms / 1e3), "hops_per_query": float(hops.mean()),
             "bytes_per_step": step_bytes, "clocks": clk}
 
@@ -511,7 +514,7 @@ def _run_ours(args, rank, world, local):
                    "beam_width": (tuned["beam_width"] if tuned else args.beam) if head != "plain" else 1,
                    "autotune": tuned,
                    "l2": "flushed (256 MB write) before every step", "parallelism": f"replicas x{world}"},
-        "recall": r["recall"], "recall_target": args.recall,
+        "recall": r["recall"], "recall_unique": r["recall_unique"], "recall_target": args.recall,
         "hops_per_query": r["hops_per_query"],
         "gathered_bytes_per_query": r["bytes_per_step"] / nq,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -524,7 +527,8 @@ def _run_ours(args, rank, world, local):
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": runner.launches_per_step * args.steps,
         "clocks": r["clocks"],
-        "forms": {f: {"qps": v["qps"], "L": v["L"], "recall": v["recall"], "ms_per_step": v["total_ms"] / args.steps,
+        "forms": {f: {"qps": v["qps"], "L": v["L"], "recall": v["recall"], "recall_unique": v["recall_unique"],
+                      "ms_per_step": v["total_ms"] / args.steps,
                       "hops_per_query": v["hops_per_query"], "gathered_bytes_per_query": v["bytes_per_step"] / nq}
                   for f, v in res.items()},
         "build_s": meta.get("build_s"),
