@@ -108,7 +108,7 @@ int gann_batch_graph_destroy(gann_batch_graph_t* g) {
   int prev = -1;
   cudaGetDevice(&prev);
   cudaSetDevice(g->device);
-  cudaStreamSynchronize(g->stream);
+  cudaDeviceSynchronize();  // a replay may run on a caller's stream
   release(g);
   if (prev >= 0) cudaSetDevice(prev);
   return GANN_OK;

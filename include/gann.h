@@ -225,7 +225,8 @@ int gann_batch_graph_create(gann_t* h, int max_nq, int topk_max, int ef_max, con
                             gann_batch_graph_t** out);
 /* Enqueue one replay on `stream` (a cudaStream_t; NULL = the graph's own stream). */
 int gann_batch_graph_launch(gann_batch_graph_t* g, void* stream);
-/* Wait for the graph's own stream and release the graph and its scratch. NULL is accepted. */
+/* Wait for the device (replays may be on any stream) and release the graph and
+ * its scratch. NULL is accepted. */
 int gann_batch_graph_destroy(gann_batch_graph_t* g);
 
 /* PQ distance tables of nq host queries (tables: nq x M x 256 FP32, host),
