@@ -244,6 +244,17 @@ __device__ __forceinline__ float adc(const TabT* table, const uint8_t* code, int
   return d;
 }
 
+// adc for M == 32 from the code's two 16-byte words, loaded ahead: the same
+// sequential sum in chunk order.
+template <class TabT>
+__device__ __forceinline__ float adc32_seq(const TabT* table, const uint4& a, const uint4& b) {
+  const uint32_t w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+  float d = 0.0f;
+#pragma unroll
+  for (int j = 0; j < 32; j++) d = __fadd_rn(d, load_tab(table, j * kPivots + ((w[j >> 2] >> (8 * (j & 3))) & 0xffu)));
+  return d;
+}
+
 // retset_push_32 (src/impl/util.cuh:116-163) by its result: the value goes
 // after every entry with distance <= value; the list keeps at most k entries.
 __device__ __forceinline__ void topk_push(float* td, int32_t* ti, int& size, int k, float value, int vid,

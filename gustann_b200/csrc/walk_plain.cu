@@ -106,22 +106,53 @@ __device__ void search_query(const PlainParams& p, const WarpSmem& s, int qid, i
     }
     const uint8_t* node = record_at(p.ix, u / p.npp, (u % p.npp) * p.node_len, u);
     const int32_t* meta = reinterpret_cast<const int32_t*>(node + p.data_len);
+    // The neighbour slots (the record holds max_m of them) load with the
+    // degree word, so a hop costs one round trip for the record and one for
+    // the codes.
+    const int e0 = lane < max_m ? __ldg(meta + 1 + lane) : -1;
+    const int e1 = lane + 32 < max_m ? __ldg(meta + 1 + lane + 32) : -1;
     const int deg = __ldg(meta);
     if (deg < 0 || deg > max_m) {
       if (lane == 0) atomicOr(p.err, kErrBadDegree);
       break;
     }
-    // ADC of every neighbour (pure_mem.cuh:294-310).
+    // ADC of every neighbour (pure_mem.cuh:294-310), each a sequential FP32
+    // sum in chunk order.
     bool bad = false;
-    for (int t = lane; t < deg; t += 32) {
-      int v = __ldg(meta + 1 + t);
-      float d = inf_f();
-      if ((unsigned)v < (unsigned)p.n)
-        d = adc(s.table, p.ix.codes + (size_t)v * M, M);
-      else
-        bad = true;
-      s.new_id[t] = (uint32_t)v;
-      s.new_d[t] = d;
+    if (M == 32 && max_m <= 64) {  // both code words of both neighbours of a lane in flight at once
+      const bool h0 = lane < deg, h1 = lane + 32 < deg;
+      const bool ok0 = h0 && (unsigned)e0 < (unsigned)p.n, ok1 = h1 && (unsigned)e1 < (unsigned)p.n;
+      bad = (h0 && !ok0) || (h1 && !ok1);
+      uint4 a0 = make_uint4(0, 0, 0, 0), b0 = a0, a1 = a0, b1 = a0;
+      if (ok0) {
+        const uint4* c = reinterpret_cast<const uint4*>(p.ix.codes + (size_t)e0 * 32);
+        a0 = __ldg(c);
+        b0 = __ldg(c + 1);
+      }
+      if (ok1) {
+        const uint4* c = reinterpret_cast<const uint4*>(p.ix.codes + (size_t)e1 * 32);
+        a1 = __ldg(c);
+        b1 = __ldg(c + 1);
+      }
+      if (h0) {
+        s.new_id[lane] = (uint32_t)e0;
+        s.new_d[lane] = ok0 ? adc32_seq(s.table, a0, b0) : inf_f();
+      }
+      if (h1) {
+        s.new_id[lane + 32] = (uint32_t)e1;
+        s.new_d[lane + 32] = ok1 ? adc32_seq(s.table, a1, b1) : inf_f();
+      }
+    } else {
+      for (int t = lane; t < deg; t += 32) {
+        const int v = t < 32 ? e0 : t < 64 ? e1 : __ldg(meta + 1 + t);
+        float d = inf_f();
+        if ((unsigned)v < (unsigned)p.n)
+          d = adc(s.table, p.ix.codes + (size_t)v * M, M);
+        else
+          bad = true;
+        s.new_id[t] = (uint32_t)v;
+        s.new_d[t] = d;
+      }
     }
     if (__any_sync(kFull, bad)) {
       if (lane == 0) atomicOr(p.err, kErrBadId);
