@@ -188,3 +188,17 @@ def test_record_division_is_exact(tmp_path):
                     str(ROOT / "tests" / "fastdiv_check.cpp"), "-o", str(exe)], check=True)
     r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0 and r.stdout.startswith("ok"), r.stdout + r.stderr
+
+
+def test_null_handles_are_rejected_before_device_work():
+    L = gb.lib()
+    out = ctypes.c_void_p()
+    assert L.gann_batch_graph_create(None, 1, 1, 1, None, None, None, None, None, None, None, None,
+                                     ctypes.byref(out)) == gb.GANN_EINVAL
+    assert L.gann_batch_graph_launch(None, None) == gb.GANN_EINVAL
+    assert L.gann_batch_graph_destroy(None) == gb.GANN_OK
+    n = ctypes.c_int64(0)
+    assert L.gann_cache_hot_records(None, None, 1, 10, 0, ctypes.byref(n)) == gb.GANN_EINVAL
+    assert L.gann_server_start(None, None, ctypes.byref(out)) == gb.GANN_EINVAL
+    assert L.gann_server_stop(None) == gb.GANN_OK
+    assert "null" in L.gann_last_error().decode()

@@ -66,3 +66,44 @@ def test_wait_for_times_out(tmp_path):
 
     with pytest.raises(TimeoutError):
         bench.wait_for(tmp_path / "never", 0.1)
+
+
+def test_calibrate_finds_smallest_L():
+    """calibrate(): walk the L ladder, then bisect to a step of 8, returning the
+    smallest L whose recall reaches the target (host logic, fake runner)."""
+    import sys
+    import types
+
+    import numpy as np
+
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    class FakeG:
+        def check(self, stream=None):
+            pass
+
+    for threshold in (37, 200, 384, 393, 1000):
+        calls = []
+
+        class Runner:
+            g = FakeG()
+
+            def run(self, L, counters=False):
+                calls.append(L)
+                # recall >= 0.95 exactly when L >= threshold
+                self.ids = types.SimpleNamespace(cpu=lambda L=L: types.SimpleNamespace(numpy=lambda: L))
+
+        orig = bench.recall_at
+        bench.recall_at = lambda ids, gt, k: 0.96 if ids >= threshold else 0.5
+        try:
+            import torch
+
+            sync = torch.cuda.synchronize
+            torch.cuda.synchronize = lambda: None
+            L, rec = bench.calibrate(Runner(), None, 10, 0.95)
+        finally:
+            bench.recall_at = orig
+            torch.cuda.synchronize = sync
+        assert rec >= 0.95 and L >= threshold and L - threshold < 8, (threshold, L, calls)
+        assert L % 8 == 0 or L in bench.L_LADDER
