@@ -240,3 +240,27 @@ def test_graph_replays_match_batch(scale):
             assert (gi[n:] == -7).all() and (gf[n:] == -7).all()
         bg.destroy()
     g.check()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["u8_nav", "f32_nav", "u8_medoid"])
+def test_batched_fp32_matches_cpu_model(golden, oracle_mod, name):
+    """With FP32 tables the batched form is deterministic: ids, distances and
+    counts equal the cache-free CPU model (tests/batch_model.py) bit for bit,
+    for every W and with visited caches far smaller than L (16 or 32 slots), so
+    the cache's evictions and the duplicate removal never change a result."""
+    from batch_model import BatchModel
+
+    meta = golden[name]
+    model = BatchModel(oracle_mod, meta)
+    g = open_meta(meta)
+    q = meta["queries"][:100]
+    for k, L, W, hb in ((10, 40, 4, 4), (10, 24, 1, 4), (5, 32, 2, 5), (10, 64, 8, 4)):
+        ids, dis, fnd, _ = g.search_batch(q, k, L, precision=gb.PREC_FP32, beam_width=W, hash_bits=hb)
+        mi, md, mf = model.search(q, k, L, W)
+        what = f"{name} k={k} L={L} W={W} hash_bits={hb}"
+        np.testing.assert_array_equal(fnd, mf, err_msg=what)
+        bad = np.nonzero((ids != mi).any(1))[0]
+        assert bad.size == 0, f"{what}: {bad.size} queries differ, first {bad[:5]}"
+        np.testing.assert_array_equal(dis.view(np.uint32), md.view(np.uint32), err_msg=what)
+    g.check()

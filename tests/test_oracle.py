@@ -133,3 +133,25 @@ def test_topk_semantics_ties_go_after(golden, oracle_mod):
         order = sorted(range(len(trace)), key=lambda i: (exact[i], i))[:10]
         assert list(ids[:fnd]) == [int(trace[i]) for i in order]
         assert list(dis[:fnd]) == [exact[i] for i in order]
+
+
+def test_batch_model_is_sane(golden, oracle_mod):
+    """The CPU model of the batched walk (tests/batch_model.py): k results in
+    ascending order, and close to the reference walk's recall on the fixture."""
+    import torch
+
+    from batch_model import BatchModel
+    from gustann_b200.indexing import formats, groundtruth
+
+    meta = golden["u8_nav"]
+    q = meta["queries"][:40]
+    model = BatchModel(oracle_mod, meta)
+    di = formats.read_disk_index(meta["index_file"], np.uint8)
+    gt = groundtruth.knn(torch.from_numpy(di.data), torch.from_numpy(q), 10)
+    o = oracle_mod.Oracle(meta["index_file"], meta["pq_prefix"], meta["nav_dir"], meta["dtype"])
+    plain = groundtruth.recall(o.search(q, 10, 40)[0], gt, 10)
+    for W in (1, 4):
+        ids, dis, fnd = model.search(q, 10, 40, W)
+        assert (fnd == 10).all()
+        assert np.all(np.diff(dis, axis=1) >= 0)
+        assert groundtruth.recall(ids, gt, 10) >= plain - 0.05
