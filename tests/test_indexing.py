@@ -1,0 +1,83 @@
+"""CPU checks of the index tooling (gustann_b200/indexing): PQ chunking and
+encoding, RobustPrune's rule, brute-force ground truth, and a small end-to-end
+build whose files the oracle searches with high recall."""
+import numpy as np
+import pytest
+import torch
+
+from gustann_b200.indexing import build_index, builder, formats, groundtruth, pq, synth
+
+
+@pytest.mark.parametrize("dim,M", [(128, 32), (96, 32), (100, 25), (20, 7), (64, 16)])
+def test_chunk_offsets_tile_the_dimensions(dim, M):
+    o = pq.chunk_offsets(dim, M).astype(np.int64)
+    sizes = np.diff(o)
+    assert o[0] == 0 and o[-1] == dim and len(o) == M + 1
+    assert sizes.min() >= 1 and sizes.max() - sizes.min() <= 1
+    assert np.all(np.diff(sizes) <= 0)  # the wider chunks come first
+
+
+def test_pq_encode_picks_the_nearest_centroid():
+    rng = np.random.default_rng(0)
+    x = rng.standard_normal((600, 16)).astype(np.float32)
+    pivots, mu, offs = pq.train(torch.from_numpy(x), 4, iters=5)
+    codes = pq.encode(torch.from_numpy(x), pivots, mu, offs)
+    r = x.astype(np.float64) - mu
+    for c in range(4):
+        b, e = int(offs[c]), int(offs[c + 1])
+        d = ((r[:, None, b:e] - pivots[None, :, b:e].astype(np.float64)) ** 2).sum(-1)
+        chosen = d[np.arange(len(x)), codes[:, c]]
+        assert np.all(chosen <= d.min(1) * (1 + 1e-4) + 1e-6)
+
+
+def test_robust_prune_rule():
+    """Kept neighbours are candidates in distance order; a candidate is dropped
+    only if an earlier kept neighbour p satisfies alpha * d(p, c) < d(u, c)."""
+    rng = np.random.default_rng(1)
+    x = torch.from_numpy(rng.standard_normal((300, 8)).astype(np.float32))
+    n, K, R, alpha = 300, 24, 6, 1.2
+    d = builder.sqdist(x, x)
+    d.fill_diagonal_(float("inf"))
+    cd, cand = torch.sort(d, 1)
+    cand, cd = cand[:, :K], cd[:, :K]
+    out = builder.robust_prune(x, cand, cd, R, alpha).numpy()
+    X = x.numpy().astype(np.float64)
+    for u in range(0, n, 7):
+        kept = [v for v in out[u] if v >= 0]
+        assert 1 <= len(kept) <= R
+        row = cand[u].tolist()
+        assert kept[0] == row[0] and kept == sorted(kept, key=row.index)
+        for c in row[: row.index(kept[-1]) + 1]:
+            if c in kept:
+                continue
+            dc = ((X[u] - X[c]) ** 2).sum()
+            assert any(alpha * ((X[p] - X[c]) ** 2).sum() < dc * (1 + 1e-4) for p in kept if row.index(p) < row.index(c))
+
+
+def test_groundtruth_matches_brute_force():
+    rng = np.random.default_rng(2)
+    base = rng.standard_normal((2000, 12)).astype(np.float32)
+    q = rng.standard_normal((30, 12)).astype(np.float32)
+    gt = groundtruth.knn(torch.from_numpy(base), torch.from_numpy(q), 10)
+    d = ((q[:, None, :].astype(np.float64) - base[None].astype(np.float64)) ** 2).sum(-1)
+    np.testing.assert_array_equal(np.asarray(gt)[:, :10], np.argsort(d, 1, kind="stable")[:, :10])
+    assert groundtruth.recall(np.asarray(gt)[:, :10], gt, 10) == 1.0
+
+
+def test_small_build_is_valid_and_searchable(tmp_path, oracle_mod):
+    base, qs = synth.make("u8", 3000, 32, 8, 60, backend="numpy")
+    f = build_index(base, str(tmp_path), R=16, M=8, nav_samples=200)
+    di = formats.read_disk_index(f.index_file, np.uint8)
+    np.testing.assert_array_equal(di.data, base)
+    assert di.R == 16 and 0 <= di.medoid < 3000
+    assert di.degrees.min() >= 1 and di.degrees.max() <= 16
+    for u in range(0, 3000, 11):
+        nb = di.graph[u, :di.degrees[u]]
+        assert np.all((nb >= 0) & (nb < 3000)) and u not in nb and len(set(nb.tolist())) == len(nb)
+    reach = builder.reachable_from(di.graph, di.degrees, di.medoid)
+    assert reach.mean() > 0.99
+    gt = groundtruth.knn(torch.from_numpy(base), torch.from_numpy(qs), 10)
+    o = oracle_mod.Oracle(f.index_file, f.pq_prefix, f.nav_dir, 0)
+    ids, dis, fnd, hops, flags, ent = o.search(qs.astype(np.float32), 10, 64)
+    assert not flags.any()
+    assert groundtruth.recall(ids, gt, 10) > 0.9
