@@ -202,3 +202,24 @@ def test_null_handles_are_rejected_before_device_work():
     assert L.gann_server_start(None, None, ctypes.byref(out)) == gb.GANN_EINVAL
     assert L.gann_server_stop(None) == gb.GANN_OK
     assert "null" in L.gann_last_error().decode()
+
+
+@pytest.mark.parametrize("cname,pycls", [("gann_batch_opts_t", "BatchOpts"), ("gann_server_opts_t", "ServerOpts"),
+                                         ("gann_load_stats_t", "LoadStats"), ("gann_info_t", "GannInfo")])
+def test_ctypes_structs_match_the_header(tmp_path, cname, pycls):
+    """Every field offset and the size of each ctypes mirror equal what a C
+    compiler lays out from include/gann.h."""
+    import subprocess
+
+    cls = getattr(gb, pycls)
+    fields = [f for f, _ in cls._fields_]
+    src = tmp_path / "layout.c"
+    src.write_text("#include <stddef.h>\n#include <stdio.h>\n#include \"gann.h\"\nint main(void) {\n"
+                   + f'  printf("%zu\\n", sizeof({cname}));\n'
+                   + "".join(f'  printf("%zu\\n", offsetof({cname}, {f}));\n' for f in fields)
+                   + "  return 0;\n}\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    assert got[0] == ctypes.sizeof(cls)
+    assert got[1:] == [getattr(cls, f).offset for f in fields]
