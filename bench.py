@@ -5,7 +5,12 @@ index of the chosen workload, at the smallest L whose recall@10 reaches the
 target (0.95). Prints one JSON line.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload c0|c1|c2|small] [--form plain]
+                    [--workload c2|c0|c1|c2_10m|small] [--forms plain,batched_bf16,...]
+
+The default workload is c2: 100M x 128 uint8 vectors (10,000-cluster mixture),
+Vamana-style graph R 32, PQ 32 x 256, a 1M-point pivot graph, all resident in
+HBM. The index is built once per box (about ten minutes, in a child process)
+and cached under --cache.
 
 Multi-GPU (torchrun, one process per GPU): every rank holds a replica of the
 index and searches its own full query batch (weak scaling, no collective on the
@@ -13,9 +18,10 @@ data path); the reported value is all ranks' queries / the slowest rank's time.
 
 --impl reference runs the reference algorithm on the host cores: the CPU
 restatement in oracle/ (bit-exact with the reference's kernel on the committed
-fixtures), over all host threads, one bounded sample of the queries per step.
-When the reference's own CUDA build (oracle/_ref) is present it is timed too and
-reported beside it.
+fixtures), over all host threads, on the same queries, at the L that the same
+calibration picks for it. When the reference's own CUDA build (oracle/_ref) is
+present it is timed too and its outputs are saved beside the workload, so that
+our arm can compare its plain form with them id for id.
 """
 from __future__ import annotations
 
@@ -40,8 +46,11 @@ WORKLOADS = {
     "c0": ("u8", 1_000_000, 128, 1_000, 64, 32, 10_000),
     "c1": ("f32", 10_000_000, 96, 4_096, 64, 32, 100_000),
     "c2": ("u8", 100_000_000, 128, 10_000, 32, 32, 1_000_000),
+    # the C2 generator and graph shape at a tenth of the size (10,000 points per cluster as in c2)
+    "c2_10m": ("u8", 10_000_000, 128, 1_000, 32, 32, 100_000),
 }
 L_LADDER = [16, 24, 32, 48, 64, 96, 128, 160, 192, 256, 320, 384, 448, 512, 640, 768, 1024, 1536, 2048]
+MIX_L, MIX_K = (32, 64, 128, 256), (1, 10, 100)
 
 
 def log(*a):
@@ -95,36 +104,106 @@ def wait_for(path: Path, seconds: float) -> None:
 
 # ----------------------------------------------------------------------------- workload preparation
 
-def prepare(workload: str, nq: int, cache: Path, rank_local: int) -> dict:
-    """Build (once per box) the index, queries and ground truth of a workload."""
+def build_workload(workload: str, nq: int, cache: Path) -> None:
+    """Build the index, queries and ground truth of a workload (runs in the
+    child process that prepare() starts)."""
+    import torch
+
+    from gustann_b200.indexing import build_index, groundtruth, synth
+
     kind, n, dim, clusters, R, M, nav = WORKLOADS[workload]
+    d = cache / f"{workload}_nq{nq}"
+    d.mkdir(parents=True, exist_ok=True)
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    t0 = time.time()
+    base, qs = synth.make(kind, n, dim, clusters, nq, backend="torch", device="cuda")
+    log(f"{workload}: data generated in {time.time() - t0:.1f} s")
+    f = build_index(base, str(d), R=R, M=M, nav_samples=nav, device="cuda", log=log)
+    t1 = time.time()
+    gt = groundtruth.knn(base, qs, 100)
+    log(f"{workload}: ground truth in {time.time() - t1:.1f} s")
+    np.save(d / "queries.npy", qs.float().cpu().numpy())
+    np.save(d / "gt.npy", gt)
+    meta = {"workload": workload, "kind": kind, "n": n, "dim": dim, "clusters": clusters, "R": R, "M": M,
+            "nav": nav, "nq": nq, "index_file": f.index_file, "pq_prefix": f.pq_prefix,
+            "nav_dir": f.nav_dir, "build_s": time.time() - t0, "timings": f.timings}
+    (d / "ready.json").write_text(json.dumps(meta))
+
+
+def prepare(workload: str, nq: int, cache: Path, rank_local: int) -> dict:
+    """The workload's files, built once per box. The build runs in a child
+    process (bench.py --prepare-only), so the calling arm maps only what it
+    measures: the reference arm never loads this repository's libraries."""
     d = cache / f"{workload}_nq{nq}"
     ready = d / "ready.json"
     if not ready.exists():
         if rank_local == 0:
-            import torch
-
-            from gustann_b200.indexing import build_index, groundtruth, synth
-
-            d.mkdir(parents=True, exist_ok=True)
-            t0 = time.time()
-            base, qs = synth.make(kind, n, dim, clusters, nq, backend="torch", device="cuda")
-            f = build_index(base, str(d), R=R, M=M, nav_samples=nav, device="cuda")
-            gt = groundtruth.knn(base, qs, 100)
-            np.save(d / "queries.npy", qs.float().cpu().numpy())
-            np.save(d / "gt.npy", gt)
-            meta = {"workload": workload, "kind": kind, "n": n, "dim": dim, "clusters": clusters, "R": R, "M": M,
-                    "nav": nav, "nq": nq, "index_file": f.index_file, "pq_prefix": f.pq_prefix,
-                    "nav_dir": f.nav_dir, "build_s": time.time() - t0, "timings": f.timings}
-            del base
-            torch.cuda.empty_cache()
-            ready.write_text(json.dumps(meta))
+            cmd = [sys.executable, str(ROOT / "bench.py"), "--prepare-only", "--workload", workload, "--nq", str(nq),
+                   "--cache", str(cache)]
+            subprocess.run(cmd, check=True, stdout=sys.stderr)
         else:
-            wait_for(ready, 3600)
+            wait_for(ready, 7200)
     meta = json.loads(ready.read_text())
+    meta["dir"] = str(d)
     meta["queries"] = np.load(d / "queries.npy")
     meta["gt"] = np.load(d / "gt.npy")
     return meta
+
+
+def config_of(meta: dict, nq: int, k: int) -> dict:
+    """The workload as both arms state it."""
+    gb = (meta["n"] * (meta["dim"] * (1 if meta["kind"] == "u8" else 4) + 4 * (meta["R"] + 1)) * 1.0
+          + meta["n"] * meta["M"]) / 1e9
+    return {"workload": meta["workload"], "n": meta["n"], "dim": meta["dim"], "vector": meta["kind"],
+            "R": meta["R"], "pq_chunks": meta["M"], "nav_points": meta["nav"], "queries_per_step": nq, "k": k,
+            "recall_target": 0.95,
+            "l2": f"inputs larger than L2: records + codes {gb:.1f} GB, gathered at random"}
+
+
+def calc_recall(ids: np.ndarray, gt: np.ndarray, k: int) -> float:
+    """calc_recall (bin/utils.hpp:105-117): every returned id found among the
+    first k ground-truth ids counts, repeated ids again."""
+    r, g = ids[:, :k], gt[:, :k]
+    return float((r[:, :, None] == g[:, None, :]).any(2).sum()) / (r.shape[0] * k)
+
+
+def recall_unique(ids: np.ndarray, gt: np.ndarray, k: int) -> float:
+    """Each distinct returned id counted once."""
+    r = np.sort(ids[:, :k], 1)
+    first = np.ones_like(r, dtype=bool)
+    first[:, 1:] = r[:, 1:] != r[:, :-1]
+    hit = (r[:, :, None] == gt[:, None, :k]).any(2) & first
+    return float(hit.sum()) / (r.shape[0] * k)
+
+
+def calibrate_L(recall_for, k: int, target: float, fixed_L: int | None = None):
+    """Smallest L (to a step of 8) whose recall@k reaches the target: walk the
+    ladder, then bisect between the last ladder value that missed and the first
+    that reached it. Both arms use this with their own recall_for(L)."""
+    if fixed_L:
+        return fixed_L, recall_for(fixed_L)
+    lo, best = None, None
+    for L in L_LADDER:
+        if L < k:
+            continue
+        r = recall_for(L)
+        best = (L, r)
+        if r >= target:
+            break
+        lo = L
+    if best is None or best[1] < target or lo is None:
+        return best
+    hi = best
+    while hi[0] - lo > 8:
+        mid = (lo + hi[0]) // 2 // 8 * 8
+        if mid <= lo:
+            break
+        r = recall_for(mid)
+        if r >= target:
+            hi = (mid, r)
+        else:
+            lo = mid
+    return hi
 
 
 # ----------------------------------------------------------------------------- clocks
@@ -177,12 +256,6 @@ class ClockSampler:
 
 
 # ----------------------------------------------------------------------------- our arm
-
-def recall_at(ids: np.ndarray, gt: np.ndarray, k: int) -> float:
-    from gustann_b200.indexing.groundtruth import recall
-
-    return recall(ids, gt, k)
-
 
 class PlainRunner:
     """gann_search_device_ex on resident device buffers (the reference-semantics form)."""
@@ -252,41 +325,15 @@ class BatchRunner(PlainRunner):
 
 
 def calibrate(runner, gt, k, target, fixed_L=None):
-    """Smallest L (to a step of 8) whose recall@k reaches the target: walk the
-    ladder, then bisect between the last ladder value that missed and the first
-    that reached it."""
     import torch
 
     def recall_for(L):
         runner.run(L)
         torch.cuda.synchronize()
         runner.g.check()
-        return recall_at(runner.ids.cpu().numpy(), gt, k)
+        return calc_recall(runner.ids.cpu().numpy(), gt, k)
 
-    if fixed_L:
-        return fixed_L, recall_for(fixed_L)
-    lo, best = None, None
-    for L in L_LADDER:
-        if L < k:
-            continue
-        r = recall_for(L)
-        best = (L, r)
-        if r >= target:
-            break
-        lo = L
-    if best is None or best[1] < target or lo is None:
-        return best
-    hi = best
-    while hi[0] - lo > 8:
-        mid = (lo + hi[0]) // 2 // 8 * 8
-        if mid <= lo:
-            break
-        r = recall_for(mid)
-        if r >= target:
-            hi = (mid, r)
-        else:
-            lo = mid
-    return hi
+    return calibrate_L(recall_for, k, target, fixed_L)
 
 
 def time_steps(runner, L, steps, warmup, world, flush):
@@ -346,7 +393,7 @@ def serving_sweep(g, meta, rates, seconds, max_batch, streams):
     q = meta["queries"]
     ks = rng.choice(np.array([1, 10, 100], np.int32), len(q)).astype(np.int32)
     Ls = np.exp(rng.uniform(np.log(32), np.log(512), len(q))).astype(np.int32)
-    srv = gb.Server(g, max_batch=max_batch, streams=streams, topk_max=100, ef_max=512, precision=gb.PREC_BF16)
+    srv = gb.Server(g, max_batch=max_batch, streams=streams, topk_max=100, ef_max=512, precision=gb.PREC_BF16X3)
     out = []
     try:
         srv.open_loop(q, rates[0], 0.2, topk=ks, ef_search=Ls, seed=99)  # warm-up
@@ -359,7 +406,7 @@ def serving_sweep(g, meta, rates, seconds, max_batch, streams):
     finally:
         srv.stop()
     return {"k": [1, 10, 100], "L": "log-uniform [32, 512]", "max_batch": max_batch, "streams": streams,
-            "seconds_per_rate": seconds, "precision": "bf16", "points": out}
+            "seconds_per_rate": seconds, "precision": "bf16x3", "points": out}
 
 
 def cpu_baseline(meta, L, k, budget_s=15.0):
@@ -420,8 +467,6 @@ def measure_form(runner, args, gt, world, flush, local, fixed_L=None):
     L, rec = calibrate(runner, gt, args.k, args.recall, fixed_L or args.L or None)
     runner.run(L, counters=True)
     torch.cuda.synchronize()
-    from gustann_b200.indexing.groundtruth import recall_unique
-
     rec_u = recall_unique(runner.ids.cpu().numpy(), gt, args.k)
     hops = runner.hops.cpu().numpy()
     step_bytes = int(runner.bytes.sum().item())
@@ -433,6 +478,112 @@ def measure_form(runner, args, gt, world, flush, local, fixed_L=None):
     return {"L": L, "recall": rec, "recall_unique": rec_u, "total_ms": total_ms, "avg_ms": float(np.mean(times_ms)),
             "qps": world * runner.nq * args.steps / (total_ms / 1e3), "hops_per_query": float(hops.mean()),
             "bytes_per_step": step_bytes, "clocks": clk}
+
+
+class MixRunner:
+    """The batching config's step: every query with its own L and k (L drawn
+    from {32, 64, 128, 256}, k from {1, 10, 100}, L raised to k), in one
+    batched launch (gann_search_batch_device with per-query arrays) or, for the
+    plain form, one gann_search_device_ex call per (L, k) group."""
+
+    def __init__(self, g, q_dev, kq: np.ndarray, Lq: np.ndarray, precision, beam_width, name, plain=False):
+        import torch
+
+        self.g, self.q, self.name, self.plain = g, q_dev, name, plain
+        self.precision, self.W = precision, beam_width
+        self.nq = q_dev.shape[0]
+        self.kq, self.Lq = kq, Lq
+        self.k_max, self.L_max = int(kq.max()), int(Lq.max())
+        if plain:
+            self.groups = []
+            for L in np.unique(Lq):
+                for k in np.unique(kq):
+                    rows = np.nonzero((Lq == L) & (kq == k))[0]
+                    if rows.size:
+                        ri = torch.from_numpy(rows).cuda()
+                        self.groups.append((int(L), int(k), rows, q_dev[ri].contiguous(),
+                                            torch.zeros((rows.size, int(k)), dtype=torch.int32, device="cuda"),
+                                            torch.zeros((rows.size, int(k)), dtype=torch.float32, device="cuda"),
+                                            torch.zeros(rows.size, dtype=torch.int32, device="cuda")))
+            self.launches_per_step = len(self.groups)
+        else:
+            self.d_k = torch.from_numpy(kq.astype(np.int32)).cuda()
+            self.d_L = torch.from_numpy(Lq.astype(np.int32)).cuda()
+            self.ids = torch.zeros((self.nq, self.k_max), dtype=torch.int32, device="cuda")
+            self.dis = torch.zeros((self.nq, self.k_max), dtype=torch.float32, device="cuda")
+            self.fnd = torch.zeros(self.nq, dtype=torch.int32, device="cuda")
+            import gustann_b200 as gb
+
+            self.launches_per_step = 2 if precision in (gb.PREC_BF16, gb.PREC_BF16X3) else 1
+
+    def run(self, L=None, counters=False):
+        import torch
+
+        s = torch.cuda.current_stream().cuda_stream
+        if self.plain:
+            for L_, k_, _, qg, ig, dg, fg in self.groups:
+                self.g.search_device_ex(qg.data_ptr(), qg.shape[0], k_, L_, ig.data_ptr(), dg.data_ptr(),
+                                        fg.data_ptr(), 0, 0, s)
+        else:
+            self.g.search_batch_device(self.q.data_ptr(), self.nq, self.d_k.data_ptr(), self.d_L.data_ptr(),
+                                       self.k_max, self.L_max, self.ids.data_ptr(), self.dis.data_ptr(),
+                                       self.fnd.data_ptr(), precision=self.precision, beam_width=self.W, stream=s)
+
+    def recall_by_k(self, gt) -> dict:
+        ids = np.zeros((self.nq, self.k_max), np.int32)
+        if self.plain:
+            for _, k_, rows, _, ig, _, _ in self.groups:
+                ids[rows, :k_] = ig.cpu().numpy()
+        else:
+            ids = self.ids.cpu().numpy()
+        return {str(k): calc_recall(ids[self.kq == k], gt[self.kq == k], int(k)) for k in np.unique(self.kq)}
+
+
+def measure_mix(g, q, gt, args, world, flush, local, W):
+    """QPS and recall@k per k of the batching config's mixed step, plain form
+    against the batched forms."""
+    import gustann_b200 as gb
+    from gustann_b200.indexing import synth
+
+    Lq, kq = synth.draws(q.shape[0], MIX_L, MIX_K)
+    out = {"L": "uniform over {32, 64, 128, 256}, raised to k", "k": "uniform over {1, 10, 100}",
+           "queries_per_step": int(q.shape[0]), "forms": {}}
+    for name, prec, plain in (("plain", None, True), ("batched_bf16", gb.PREC_BF16, False),
+                              ("batched_bf16x3", gb.PREC_BF16X3, False)):
+        r = MixRunner(g, q, kq, Lq, prec, W, name, plain)
+        r.run()
+        times = time_steps(r, None, args.steps, args.warmup, world, flush)
+        total_ms = max_over_ranks(float(sum(times)), world, device="cuda")
+        out["forms"][name] = {"qps": world * r.nq * args.steps / (total_ms / 1e3),
+                              "ms_per_step": total_ms / args.steps, "recall_at_k": r.recall_by_k(gt),
+                              "launches_per_step": r.launches_per_step}
+    out["speedup_vs_plain"] = out["forms"]["batched_bf16"]["qps"] / out["forms"]["plain"]["qps"]
+    return out
+
+
+def plain_parity(g, meta, q_dev, k):
+    """The plain form against the reference kernel's own outputs on the same
+    index and queries (saved by the reference arm), id for id."""
+    import torch
+
+    p = Path(meta["dir"]) / f"ref_kernel_k{k}.npz"
+    if not p.exists():
+        return None
+    r = np.load(p)
+    L, rows = int(r["L"]), r["rows"]
+    runner = PlainRunner(g, q_dev, k)
+    runner.run(L)
+    torch.cuda.synchronize()
+    g.check()
+    ids, dis, fnd = (runner.ids.cpu().numpy()[rows], runner.dis.cpu().numpy()[rows], runner.fnd.cpu().numpy()[rows])
+    same = (ids == r["ids"]).all(1)
+    return {"against": "the reference's search_graph_kernel_gpumem + nav kernel (oracle/_ref), run by the "
+                       "reference arm on the same index files and queries",
+            "L": L, "k": k, "queries": int(rows.size), "skipped_by_screen": int(q_dev.shape[0] - rows.size),
+            "plain_ids_equal": float(same.mean()) if rows.size else None,
+            "id_rows_differing": int((~same).sum()),
+            "dist_bit_mismatches": int((dis.view(np.uint32) != r["dists"].view(np.uint32)).sum()),
+            "found_mismatches": int((fnd != r["found"]).sum())}
 
 
 def _run_ours(args, rank, world, local):
@@ -447,7 +598,9 @@ def _run_ours(args, rank, world, local):
     barrier(world)
     dtype = gb.DataType.UINT8 if meta["kind"] == "u8" else gb.DataType.FLOAT
     g = gb.GustANN(dtype)
+    t_open = time.time()
     g.init_pure_mem(gb.GustANNConfig(meta["index_file"], meta["pq_prefix"], meta["nav_dir"] or ""))
+    open_s = time.time() - t_open
     q = torch.from_numpy(meta["queries"]).cuda()
     gt = meta["gt"]
     k = args.k
@@ -455,8 +608,11 @@ def _run_ours(args, rank, world, local):
                "batched_bf16": BatchRunner(g, q, k, gb.PREC_BF16, args.beam, "batched_bf16"),
                "batched_bf16x3": BatchRunner(g, q, k, gb.PREC_BF16X3, args.beam, "batched_bf16x3"),
                "batched_fp32": BatchRunner(g, q, k, gb.PREC_FP32, args.beam, "batched_fp32")}
+    forms_arg = args.forms or ("plain,batched_bf16,batched_bf16x3,batched_fp32" if meta["n"] > 2_000_000 else
+                               "plain,batched_bf16,batched_bf16x3,batched_fp32,host_plain,host_batched_bf16,"
+                               "host_batched_bf16_cached")
     gh = None
-    if any(f.startswith("host_") for f in args.forms.split(",")):
+    if any(f.startswith("host_") for f in forms_arg.split(",")):
         # records in pinned host memory (use_gpu_mem = false), read over PCIe/C2C
         gh = gb.GustANN(dtype)
         gh.init_pure_mem(gb.GustANNConfig(meta["index_file"], meta["pq_prefix"], meta["nav_dir"] or ""),
@@ -464,7 +620,7 @@ def _run_ours(args, rank, world, local):
         runners["host_plain"] = PlainRunner(gh, q, k)
         runners["host_batched_bf16"] = BatchRunner(gh, q, k, gb.PREC_BF16, args.beam, "host_batched_bf16")
     gc, cache_info = None, None
-    if "host_batched_bf16_cached" in args.forms.split(","):
+    if "host_batched_bf16_cached" in forms_arg.split(","):
         # host-memory records plus an HBM cache of the hottest ones, chosen by a
         # sample batch of base vectors (not the timed queries)
         from gustann_b200.indexing import formats
@@ -482,7 +638,7 @@ def _run_ours(args, rank, world, local):
                       "sample": f"{sample.shape[0]} base vectors at L {args.tune_L}"}
         runners["host_batched_bf16_cached"] = BatchRunner(gc, q, k, gb.PREC_BF16, args.beam,
                                                           "host_batched_bf16_cached")
-    forms = [f for f in args.forms.split(",") if f in runners]
+    forms = [f for f in forms_arg.split(",") if f in runners]
     tuned = None
     if args.beam == 0 and any(f != "plain" for f in forms):  # autotuner: beam width and visited cache
         W, hb, secs = g.autotune(q.data_ptr(), q.shape[0], k, args.tune_L, gb.PREC_BF16)
@@ -492,6 +648,7 @@ def _run_ours(args, rank, world, local):
     for f in forms:  # a host-paged form runs at the L of its HBM twin (same results, same recall)
         twin = res.get(f[5:].replace("_cached", "")) if f.startswith("host_") else None
         res[f] = measure_form(runners[f], args, gt, world, flush, local, twin["L"] if twin else None)
+        log(f"{f}: L {res[f]['L']} recall {res[f]['recall']:.4f} qps {res[f]['qps']:.0f}")
     ok = [f for f in forms if res[f]["recall"] >= args.recall and not f.startswith("host_")]
     head = args.headline if args.headline in ok else (max(ok, key=lambda f: res[f]["qps"]) if ok else forms[0])
     r, runner = res[head], runners[head]
@@ -508,12 +665,10 @@ def _run_ours(args, rank, world, local):
         "scaling": "weak", "vs_baseline": None, "dtype": "bf16" if "bf16" in head else "f32",
         "data": f"synthetic seeded Gaussian mixture ({meta['clusters']} clusters) standing in for "
                 f"{'SIFT' if meta['kind'] == 'u8' else 'DEEP'}; index built on the device",
-        "config": {"workload": args.workload, "n": meta["n"], "dim": meta["dim"], "vector": meta["kind"],
-                   "R": meta["R"], "pq_chunks": meta["M"], "nav_points": meta["nav"], "queries_per_step": nq,
-                   "k": k, "L": r["L"], "form": head,
-                   "beam_width": (tuned["beam_width"] if tuned else args.beam) if head != "plain" else 1,
-                   "autotune": tuned,
-                   "l2": "flushed (256 MB write) before every step", "parallelism": f"replicas x{world}"},
+        "config": config_of(meta, nq, k),
+        "form": head, "L": r["L"], "parallelism": f"replicas x{world}",
+        "beam_width": (tuned["beam_width"] if tuned else args.beam) if head != "plain" else 1, "autotune": tuned,
+        "l2_flush": "256 MB write before every GPU step, outside the timed span",
         "recall": r["recall"], "recall_unique": r["recall_unique"], "recall_target": args.recall,
         "hops_per_query": r["hops_per_query"],
         "gathered_bytes_per_query": r["bytes_per_step"] / nq,
@@ -531,11 +686,16 @@ def _run_ours(args, rank, world, local):
                       "ms_per_step": v["total_ms"] / args.steps,
                       "hops_per_query": v["hops_per_query"], "gathered_bytes_per_query": v["bytes_per_step"] / nq}
                   for f, v in res.items()},
-        "build_s": meta.get("build_s"),
+        "build_s": meta.get("build_s"), "build_timings": meta.get("timings"), "open_s": open_s,
         "host_record_cache": cache_info,
     }
     if "plain" in res and head != "plain":
         out["speedup_vs_plain"] = r["qps"] / res["plain"]["qps"]
+    par = plain_parity(g, meta, q, k)
+    if par is not None:
+        out["parity"] = par
+    if args.mix:
+        out["mix"] = measure_mix(g, q, gt, args, world, flush, local, args.beam)
     if world == 1 and args.serve_rates:
         rates = [float(x) for x in args.serve_rates.split(",") if x]
         out["serving"] = serving_sweep(g, meta, rates, args.serve_seconds, args.serve_batch, args.serve_streams)
@@ -559,6 +719,10 @@ def _run_ours(args, rank, world, local):
 # ----------------------------------------------------------------------------- reference arm
 
 def run_reference(args, rank, world, local):
+    """The reference algorithm on the host cores (the oracle), on this arm's
+    workload, queries, k and the L the shared calibration picks; and the
+    reference's own CUDA kernel on the screened queries, whose outputs are saved
+    for our arm's id-for-id comparison. This process maps only oracle/ libraries."""
     if rank != 0:
         return
     import torch
@@ -570,98 +734,95 @@ def run_reference(args, rank, world, local):
     dtype = 0 if meta["kind"] == "u8" else 1
     k = args.k
     q, gt = meta["queries"], meta["gt"]
+    nq = q.shape[0]
     o = Oracle(meta["index_file"], meta["pq_prefix"], meta["nav_dir"], dtype)
     cores = max_threads()
-    # L for the recall target, with the reference algorithm itself (on a subsample)
-    sub = min(len(q), 1000)
-    L = args.L
-    if not L:
-        for L in L_LADDER:
-            if L < k:
-                continue
-            ids, *_ = o.search(q[:sub], k, L, threads=cores)
-            if recall_at(ids, gt[:sub], k) >= args.recall:
-                break
-    probe = min(len(q), max(64, cores * 8))
+
+    def recall_for(L):
+        ids, *_ = o.search(q, k, L, threads=cores)
+        return calc_recall(ids, gt, k)
+
+    t_cal = time.time()
+    L, rec_cal = calibrate_L(recall_for, k, args.recall, args.L or None)
+    cal_s = time.time() - t_cal
+    probe = min(nq, max(64, cores * 8))
     o.search(q[:probe], k, L, threads=cores)
     rate = probe / max(o.last_seconds, 1e-6)
-    total_budget = 120.0
-    per_step = total_budget / max(1, args.steps + args.warmup)
-    sample = int(min(len(q), max(probe, rate * per_step)))
+    per_step = args.ref_budget / max(1, args.steps + args.warmup)
+    sample = int(min(nq, max(probe, rate * per_step)))
     for _ in range(args.warmup):
         o.search(q[:sample], k, L, threads=cores)
     secs = []
     for _ in range(args.steps):
         ids, *_ = o.search(q[:sample], k, L, threads=cores)
         secs.append(o.last_seconds)
+    o.close()
     value = sample * args.steps / sum(secs)
-    rec = recall_at(ids, gt[:sample], k)
     out = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(secs) / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic seeded Gaussian mixture; same index files as the GPU arm",
-        "config": {"workload": args.workload, "n": meta["n"], "dim": meta["dim"], "vector": meta["kind"],
-                   "R": meta["R"], "pq_chunks": meta["M"], "queries_per_step": sample, "k": k, "L": L,
-                   "form": "reference algorithm on host cores"},
-        "recall": rec,
+        "config": config_of(meta, sample, k),
+        "form": "reference algorithm on host cores", "L": L, "calibration_s": cal_s,
+        "recall": calc_recall(ids, gt[:sample], k), "recall_all_queries": rec_cal,
         "cpu_baseline": {"value": value, "unit": "queries/s", "cores": cores, "kind": "port",
-                         "sample": f"first {sample} of {len(q)} queries per step, k={k}, L={L}, "
+                         "sample": f"first {sample} of {nq} queries per step, k={k}, L={L}, "
                                    f"{cores} threads, oracle/gann_oracle.c (bit-exact with the reference "
                                    f"kernel on the committed fixtures)"},
         "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     if REF_LIB.exists() and not args.no_ref_gpu:
         # The reference's own -G path built from its sources, timed by its own
-        # timer (nav + host translate + walk, src/pure_mem.cu:101-187). It is run
-        # only on queries for which the oracle shows the walk never exhausts its
-        # list below L: there the reference expands a sentinel id
-        # (src/impl/pure_mem.cuh:380-419) and reads outside the index.
-        *_, flags, _ = o.search(q, k, L, threads=cores)
-        safe = np.nonzero(flags == 0)[0]
-        o.close()
-        if safe.size:
-            r = Reference(meta["index_file"], meta["pq_prefix"], meta["nav_dir"], dtype)
-            qs = np.ascontiguousarray(q[safe])
-            r.search(qs, k, L)
-            ts = []
-            for _ in range(3):
-                ids, dis, fnd, t = r.search(qs, k, L)
-                ts.append(t)
-            out["reference_cuda_kernel"] = {
-                "value": len(qs) / float(np.median(ts)), "unit": "queries/s", "L": L, "queries": int(len(qs)),
-                "recall": recall_at(ids, gt[safe], k),
-                "note": "reference search_graph_kernel_gpumem + nav kernel compiled for sm_100a from its "
-                        "sources (oracle/build_ref.sh), its own wall-clock timer, median of 3"}
-            r.close()
-    else:
-        o.close()
+        # timer (nav + host translate + walk, src/pure_mem.cu:101-187). Reference
+        # screens every batch with the oracle: only queries whose walk never
+        # exhausts its list below L reach the kernel (there the reference expands
+        # a sentinel id, src/impl/pure_mem.cuh:380-419, and reads outside the index).
+        r = Reference(meta["index_file"], meta["pq_prefix"], meta["nav_dir"], dtype)
+        rows, ids, dis, fnd, _ = r.search(q, k, L, threads=cores)
+        ts = []
+        for _ in range(3):
+            rows, ids, dis, fnd, t = r.search(q, k, L, threads=cores)
+            ts.append(t)
+        np.savez(Path(meta["dir"]) / f"ref_kernel_k{k}.npz", L=np.int32(L), rows=rows, ids=ids, dists=dis,
+                 found=fnd)
+        out["reference_cuda_kernel"] = {
+            "value": len(rows) / float(np.median(ts)) if len(rows) else None, "unit": "queries/s", "L": L,
+            "queries": int(len(rows)), "skipped_by_screen": r.last_skipped,
+            "recall": calc_recall(ids, gt[rows], k) if len(rows) else None,
+            "note": "reference search_graph_kernel_gpumem + nav kernel compiled for sm_100a from its "
+                    "sources (oracle/build_ref.sh), its own wall-clock timer, median of 3"}
+        r.close()
     print(json.dumps(out), flush=True)
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=list(WORKLOADS), default="c0")
+    ap.add_argument("--workload", choices=list(WORKLOADS), default="c2")
+    ap.add_argument("--prepare-only", action="store_true", help="build the workload's files and exit")
     ap.add_argument("--nq", type=int, default=10_000)
     ap.add_argument("--k", type=int, default=10)
     ap.add_argument("--recall", type=float, default=0.95)
     ap.add_argument("--L", type=int, default=0, help="fixed L (skip calibration)")
     ap.add_argument("--cache", default=os.environ.get("GANN_BENCH_CACHE", "/tmp/gann_bench"))
     ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--ref-budget", type=float, default=240.0,
+                    help="seconds of host-core search in the reference arm's warm-up + timed steps")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true")
-    ap.add_argument("--forms", default="plain,batched_bf16,batched_bf16x3,batched_fp32,host_plain,host_batched_bf16,"
-                                       "host_batched_bf16_cached")
+    ap.add_argument("--forms", default="", help="comma list (default: by workload size)")
     ap.add_argument("--host-cache", type=float, default=0.1,
                     help="HBM record cache of the host_batched_bf16_cached form, as a fraction of the page bytes")
-    ap.add_argument("--headline", default="batched_bf16")
+    ap.add_argument("--headline", default="batched_bf16x3")
     ap.add_argument("--beam", type=int, default=0, help="0 = autotune (gann_autotune)")
     ap.add_argument("--tune-L", type=int, default=384)
     ap.add_argument("--batch", type=int, default=0, help="queries per step (default: all --nq)")
+    ap.add_argument("--no-mix", dest="mix", action="store_false",
+                    help="skip the mixed-L/k step of the batching config")
     ap.add_argument("--serve-rates", default="100000,500000,1000000,1500000,2000000",
                     help="offered QPS of the open-loop serving sweep ('' = skip)")
     ap.add_argument("--serve-seconds", type=float, default=1.0)
@@ -669,7 +830,9 @@ def main():
     ap.add_argument("--serve-streams", type=int, default=8)
     args = ap.parse_args()
     rank, world, local = dist_env()
-    if args.impl == "reference":
+    if args.prepare_only:
+        build_workload(args.workload, args.nq, Path(args.cache))
+    elif args.impl == "reference":
         run_reference(args, rank, world, local)
     else:
         run_ours(args, rank, world, local)

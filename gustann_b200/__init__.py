@@ -121,6 +121,7 @@ _SIGNATURES = {
     "gann_set_fma": (_I, [_P, _I, _I]),
     "gann_last_error": (ctypes.c_char_p, []),
     "gann_sample_pivots": (_I, [ctypes.c_int64, ctypes.c_int64, ctypes.c_uint32, _P]),
+    "gann_build_prune": (_I, [_P, _I, ctypes.c_int64, _I, _P, _P, ctypes.c_int64, _I, _I, ctypes.c_float, _P, _P]),
 }
 
 

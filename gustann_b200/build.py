@@ -28,7 +28,7 @@ NVCC_FLAGS = [
 EXPORTS = [
     "gann_open", "gann_close", "gann_get_info", "gann_search", "gann_search_device", "gann_search_device_ex", "gann_search_batch", "gann_search_batch_device", "gann_search_batch_noalloc", "gann_pq_tables", "gann_autotune", "gann_server_start", "gann_server_submit", "gann_server_poll", "gann_server_stop", "gann_server_open_loop", "gann_check",
     "gann_set_fma", "gann_last_error", "gann_sample_pivots", "gann_batch_graph_create",
-    "gann_batch_graph_launch", "gann_batch_graph_destroy", "gann_cache_hot_records",
+    "gann_batch_graph_launch", "gann_batch_graph_destroy", "gann_cache_hot_records", "gann_build_prune",
 ]
 
 
@@ -97,10 +97,15 @@ def build_lib(verbose: bool = False, force: bool = False) -> Path:
     return LIB
 
 
-def build_oracle(verbose: bool = False) -> None:
-    """Build the CPU oracle, and the reference's own path when its sources exist (checker only)."""
+def build_oracle(verbose: bool = False, ref_dir: str | None = None) -> None:
+    """Build the CPU oracle, and the reference's own path when its sources exist
+    (checker only). The reference checkout is ``ref_dir`` or $GANN_REF_DIR;
+    without either only the oracle is built."""
     subprocess.run(["make", "-s", "-C", str(ROOT / "oracle")], check=True)
-    ref = Path(os.environ.get("GANN_REF_DIR", "/root/reference"))
+    ref_dir = ref_dir or os.environ.get("GANN_REF_DIR")
+    if not ref_dir:
+        return
+    ref = Path(ref_dir)
     out = ROOT / "oracle" / "_ref" / "libgustann_ref.so"
     script = ROOT / "oracle" / "build_ref.sh"
     if (ref / "src" / "pure_mem.cu").exists():
@@ -114,5 +119,5 @@ def build_oracle(verbose: bool = False) -> None:
 if __name__ == "__main__":
     build_lib(verbose="-v" in sys.argv, force="-f" in sys.argv)
     build_cli(verbose="-v" in sys.argv, force="-f" in sys.argv)
-    build_oracle(verbose="-v" in sys.argv)
+    build_oracle(verbose="-v" in sys.argv, ref_dir=next((a for a in sys.argv[1:] if not a.startswith("-")), None))
     print(LIB)

@@ -58,7 +58,7 @@ int gann_batch_graph_create(gann_t* h, int max_nq, int topk_max, int ef_max, con
     return gann_internal_set_error(GANN_ERANGE, "topk and ef_search are limited to 4096");
   if (!d_queries || !d_nq || !d_nns || !d_distances || !d_found_cnt)
     return gann_internal_set_error(GANN_EINVAL, "null buffer");
-  const int prec = opts ? opts->precision : GANN_PREC_BF16;
+  const int prec = opts ? opts->precision : GANN_PREC_BF16X3;
   int prev = -1;
   cudaGetDevice(&prev);
   cudaSetDevice(h->device);

@@ -424,12 +424,6 @@ int gann_search(gann_t* h, const float* queries, int nq, int topk, int ef_search
 
 namespace {
 
-int batch_hash_bits(int ef_max) {
-  int b = 9;
-  while ((1 << b) < 4 * ef_max && b < 13) b++;
-  return b;
-}
-
 // Enqueue one batched search. counter / tables: caller-owned work counter and
 // BF16 table buffer (nq x M x 256) for concurrent launches; null = the handle's.
 int enqueue_batch(gann_t* h, const float* d_q, int nq, const int32_t* d_k, const int32_t* d_l, int k_max,
@@ -439,11 +433,11 @@ int enqueue_batch(gann_t* h, const float* d_q, int nq, const int32_t* d_k, const
                   int32_t* visit_count = nullptr) {
   gann_batch_opts_t o{};
   if (opts) o = *opts;
-  const int prec = opts ? o.precision : GANN_PREC_BF16;
+  const int prec = opts ? o.precision : GANN_PREC_BF16X3;
   const int W = o.beam_width ? o.beam_width : (h->tuned_beam ? h->tuned_beam : 4);
   if (!(W == 1 || W == 2 || W == 4 || W == 8)) return set_error(GANN_EINVAL, "beam_width must be 1, 2, 4 or 8");
   if (prec < GANN_PREC_FP32 || prec > GANN_PREC_BF16_CC) return set_error(GANN_EINVAL, "unknown precision");
-  const int hb = o.hash_bits ? o.hash_bits : batch_hash_bits(l_max) + h->tuned_hash_delta;
+  const int hb = o.hash_bits ? o.hash_bits : gann::batch_hash_bits(l_max) + h->tuned_hash_delta;
   if (hb < 4 || hb > 16) return set_error(GANN_EINVAL, "hash_bits must be in 4..16");
   const bool bf16 = prec != GANN_PREC_FP32;
   const size_t smem = gann::batch_smem_bytes(h->hx.pq_m, bf16 ? 2 : 4, hb, l_max, (int)h->hx.max_m0, W, k_max,
@@ -658,7 +652,7 @@ int gann_autotune(gann_t* h, const float* d_queries, int nq, int topk, int ef_se
   if (e == cudaSuccess) {
     std::lock_guard<std::mutex> lk(h->mu);
     cudaStream_t s = h->stream;
-    const int base_bits = batch_hash_bits(ef_search);
+    const int base_bits = gann::batch_hash_bits(ef_search);
     for (int W : {2, 4, 8}) {
       for (int delta : {-1, 0, 1}) {
         gann_batch_opts_t o{};

@@ -154,6 +154,15 @@ struct BatchParams {
   unsigned int* err;
 };
 
+// Visited-cache size (log2 slots) of the batched form for a list of ef_max:
+// the smallest power of two >= 4 ef_max, within 2^9 .. 2^13 (the handle's tuned
+// delta is added by the caller).
+inline int batch_hash_bits(int ef_max) {
+  int b = 9;
+  while ((1 << b) < 4 * ef_max && b < 13) b++;
+  return b;
+}
+
 size_t batch_smem_bytes(int M, int tab_bytes, int hash_bits, int L_max, int max_m, int W, int k_max, int dim);
 cudaError_t launch_batch(const BatchParams& p, int dtype, int table_bf16, int W, int num_sms, cudaStream_t stream);
 

@@ -15,9 +15,12 @@
 // find the previous call's contents in it, so each call clears the work
 // counter before its kernels run; calls whose kernels overlap on the GPU (two
 // streams, or two handles on one device) race on it and must be serialised by
-// the caller. The first call on a device looks up the array's device address
-// (cudaGetSymbolAddress, with that device current); make that first call before
-// any stream capture.
+// the caller. Only the tensor-core precisions use the table region, so only
+// they are limited to kNoAllocMaxQueries queries per call. Every call looks up
+// the array's device address (cudaGetSymbolAddress, with the handle's device
+// current; it allocates nothing), so an address never outlives the context it
+// came from. The first call on a device may load the library's device code;
+// make that first call before any stream capture.
 #include <mutex>
 #include <string>
 
@@ -34,23 +37,8 @@ constexpr size_t kNoAllocBytes =
 
 static __device__ __align__(256) uint8_t g_noalloc_scratch[kNoAllocBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-void* g_scratch_addr[kMaxDevices] = {};  // device address of g_noalloc_scratch, per device
-
-// Device address of the scratch array on `device` (which must be current).
-cudaError_t scratch_address(int device, void** out) {
-  std::lock_guard<std::mutex> lk(g_mu);
-  if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
-  if (!g_scratch_addr[device]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess) return e;
-    g_scratch_addr[device] = p;
-  }
-  *out = g_scratch_addr[device];
-  return cudaSuccess;
-}
+// Device address of the scratch array on the current device.
+cudaError_t scratch_address(void** out) { return cudaGetSymbolAddress(out, g_noalloc_scratch); }
 
 }  // namespace
 }  // namespace gann
@@ -69,34 +57,33 @@ extern "C" int gann_search_batch_noalloc(gann_t* h, const float* d_queries, int 
   if (!d_queries || !d_nns || !d_distances || !d_found_cnt) return gann_internal_set_error(GANN_EINVAL, "null buffer");
   gann_batch_opts_t o{};
   if (opts) o = *opts;
-  const int prec = opts ? o.precision : GANN_PREC_BF16;
-  const int W = o.beam_width ? o.beam_width : 4;
+  const int prec = opts ? o.precision : GANN_PREC_BF16X3;
+  std::lock_guard<std::mutex> lk(h->mu);
+  // The same defaults as gann_search_batch_device: the handle's tuned beam
+  // width and visited-cache delta (gann_autotune) when the options leave 0.
+  const int W = o.beam_width ? o.beam_width : (h->tuned_beam ? h->tuned_beam : 4);
   if (!(W == 1 || W == 2 || W == 4 || W == 8)) return gann_internal_set_error(GANN_EINVAL, "beam_width must be 1, 2, 4 or 8");
   if (prec < GANN_PREC_FP32 || prec > GANN_PREC_BF16_CC) return gann_internal_set_error(GANN_EINVAL, "unknown precision");
   const bool tc = prec == GANN_PREC_BF16 || prec == GANN_PREC_BF16X3;
-  if (nq > kNoAllocMaxQueries)
-    return gann_internal_set_error(GANN_ERANGE, "gann_search_batch_noalloc: at most 512 queries per call");
+  if (tc && nq > kNoAllocMaxQueries)
+    return gann_internal_set_error(GANN_ERANGE,
+                                   "gann_search_batch_noalloc: at most 512 queries per call with tensor-core tables");
   if (tc && h->hx.pq_m > kNoAllocMaxChunks)
     return gann_internal_set_error(GANN_ERANGE, "gann_search_batch_noalloc: at most 32 PQ chunks with tensor-core tables");
   if (tc && !h->dx.tc_bpanel_hi)
     return gann_internal_set_error(GANN_ERANGE, "tensor-core tables need PQ chunks of at most 16 dimensions");
-  int hb = o.hash_bits;
-  if (!hb) {
-    hb = 9;
-    while ((1 << hb) < 4 * ef_search && hb < 13) hb++;
-  }
+  const int hb = o.hash_bits ? o.hash_bits : batch_hash_bits(ef_search) + h->tuned_hash_delta;
   if (hb < 4 || hb > 16) return gann_internal_set_error(GANN_EINVAL, "hash_bits must be in 4..16");
   if (batch_smem_bytes(h->hx.pq_m, tc || prec == GANN_PREC_BF16_CC ? 2 : 4, hb, ef_search, (int)h->hx.max_m0, W,
                        topk, (int)h->hx.dim) > 227 * 1024)
     return gann_internal_set_error(GANN_ERANGE, "table + lists + visited cache of one query exceed 227 KB of shared memory");
 
-  std::lock_guard<std::mutex> lk(h->mu);
   int prev = -1;
   if (cudaGetDevice(&prev) != cudaSuccess) return gann_internal_set_error(GANN_ECUDA, "cudaGetDevice failed");
   if (prev != h->device && cudaSetDevice(h->device) != cudaSuccess)
     return gann_internal_set_error(GANN_ECUDA, "cannot make the handle's device current");
   void* base = nullptr;
-  cudaError_t e = scratch_address(h->device, &base);
+  cudaError_t e = scratch_address(&base);
   cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
   int* counter = static_cast<int*>(base);
   __nv_bfloat16* tables = reinterpret_cast<__nv_bfloat16*>(static_cast<uint8_t*>(base) + kNoAllocHeader);

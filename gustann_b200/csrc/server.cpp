@@ -269,7 +269,7 @@ int gann_server_start(gann_t* h, const gann_server_opts_t* opts, gann_server_t**
   if (!o.topk_max) o.topk_max = 100;
   if (!o.ef_max) o.ef_max = 512;
   if (!o.max_wait_us) o.max_wait_us = 100;
-  if (!opts) o.precision = GANN_PREC_BF16;
+  if (!opts) o.precision = GANN_PREC_BF16X3;
   if (o.max_batch < 1 || o.streams < 1 || o.streams > 64 || o.topk_max < 1 || o.ef_max < 1 || o.topk_max > 4096 ||
       o.ef_max > 4096 || o.max_wait_us < 0)
     return gann_internal_set_error(GANN_EINVAL, "bad server options");

@@ -42,9 +42,14 @@ def _np(x):
 
 def build_index(base, out_dir: str, R: int, M: int = 32, alpha: float = 1.2, nav_samples: int | None = None,
                 nav_R: int = 32, device=None, n_coarse: int | None = None, nprobe: int = 4,
-                pq_train: int = 1 << 18, seed: int = 7, legacy_pq: bool = False) -> IndexFiles:
+                pq_train: int = 1 << 18, seed: int = 7, legacy_pq: bool = False, method: str = "auto",
+                leaf: int = 4096, log=None) -> IndexFiles:
     """Build and write every file of one index. ``base`` is an n x dim uint8 or
-    float32 array/tensor. ``nav_samples`` = 0 writes no pivot graph."""
+    float32 array/tensor. ``nav_samples`` = 0 writes no pivot graph.
+
+    ``method``: "vamana" (builder.build: Vamana searches from the medoid),
+    "ivf" (ivf.build: exact leaf neighbourhoods, pruned, reverse edges, the
+    pivot graph embedded as long edges) or "auto" (ivf from 4M points on)."""
     from .. import sample_pivots
 
     t0 = time.time()
@@ -55,22 +60,10 @@ def build_index(base, out_dir: str, R: int, M: int = 32, alpha: float = 1.2, nav
         x = x.to(device)
     n, dim = x.shape
     kind = "u8" if x.dtype == torch.uint8 else "f32"
-    g, deg, med = builder.build(x, R, alpha, n_coarse=n_coarse, nprobe=nprobe, seed=seed)
-    timings["graph_s"] = time.time() - t0
-    t1 = time.time()
-    pivots, centroid, offs = pq.train(x, M, n_train=pq_train, seed=seed + 4)
-    codes = pq.encode(x, pivots, centroid, offs)
-    timings["pq_s"] = time.time() - t1
-    t2 = time.time()
-    index_file = os.path.join(out_dir, "index_disk.index")
-    pq_prefix = os.path.join(out_dir, "index_pq")
-    data_np = _np(x)
-    formats.write_disk_index(index_file, data_np, g, deg, med, R)
-    formats.write_pq(pq_prefix, pivots, centroid, offs, codes, legacy=legacy_pq)
-    timings["write_s"] = time.time() - t2
-    nav_dir = None
+    large = method == "ivf" or (method == "auto" and n >= 4_000_000)
     if nav_samples is None:
         nav_samples = max(64, n // 100)
+    nav = None
     if nav_samples:
         t3 = time.time()
         ids = sample_pivots(n, min(nav_samples, n))
@@ -78,8 +71,44 @@ def build_index(base, out_dir: str, R: int, M: int = 32, alpha: float = 1.2, nav
         ng, ndeg, nmed = builder.build(sub, nav_R, alpha, seed=seed + 1)
         if int(ndeg.min()) < 3:
             raise RuntimeError("pivot graph has a node with fewer than 3 neighbours")
+        nav = (ids, sub, ng, ndeg, nmed)
+        timings["nav_s"] = time.time() - t3
+        if log:
+            log(f"pivot graph: {len(ids)} points, {timings['nav_s']:.1f} s")
+    t1 = time.time()
+    index_file = os.path.join(out_dir, "index_disk.index")
+    if large:
+        from . import ivf
+
+        g, deg, med, gt = ivf.build(x, R, alpha, seed=seed, leaf=leaf,
+                                    pivots=nav[0] if nav else None, nav_graph=nav[2] if nav else None, log=log)
+        timings.update({f"graph_{k}": v for k, v in gt.items()})
+        timings["graph_s"] = time.time() - t1
+        t2 = time.time()
+        formats.write_disk_index_torch(index_file, x, g, deg, med, R)
+        del g, deg
+        timings["write_index_s"] = time.time() - t2
+    else:
+        g, deg, med = builder.build(x, R, alpha, n_coarse=n_coarse, nprobe=nprobe, seed=seed)
+        timings["graph_s"] = time.time() - t1
+        t2 = time.time()
+        formats.write_disk_index(index_file, _np(x), g, deg, med, R)
+        timings["write_index_s"] = time.time() - t2
+    if log:
+        log(f"graph + index file: {time.time() - t1:.1f} s")
+    t1 = time.time()
+    pivots, centroid, offs = pq.train(x, M, n_train=pq_train, seed=seed + 4)
+    codes = pq.encode(x, pivots, centroid, offs)
+    pq_prefix = os.path.join(out_dir, "index_pq")
+    formats.write_pq(pq_prefix, pivots, centroid, offs, codes, legacy=legacy_pq)
+    del codes
+    timings["pq_s"] = time.time() - t1
+    nav_dir = None
+    if nav:
+        ids, sub, ng, ndeg, nmed = nav
         nav_dir = os.path.join(out_dir, "nav")
         formats.write_nav(nav_dir, _np(sub), ng, ndeg, nmed, ids)
-        timings["nav_s"] = time.time() - t3
     timings["total_s"] = time.time() - t0
+    if log:
+        log(f"index built in {timings['total_s']:.1f} s: {timings}")
     return IndexFiles(index_file, pq_prefix, nav_dir, n, dim, kind, R, M, med, timings)

@@ -130,9 +130,16 @@ def knn_candidates(x: torch.Tensor, K: int, n_coarse: int | None = None, nprobe:
 
 
 def robust_prune(x: torch.Tensor, cand: torch.Tensor, cand_d: torch.Tensor, R: int, alpha: float,
-                 batch: int = 8192) -> torch.Tensor:
+                 batch: int = 8192, rows: torch.Tensor | None = None) -> torch.Tensor:
     """RobustPrune over rows of candidates sorted by distance (-1 = none).
-    Returns n x R int64 neighbour ids (-1 padded), kept in candidate order."""
+    Returns n x R int64 neighbour ids (-1 padded), kept in candidate order.
+    On the GPU, given the rows' point ids, the same rule runs in the
+    gann_build_prune kernel (which re-scores the candidates exactly and orders
+    ties by id, as the sorted rows here are)."""
+    if x.is_cuda and rows is not None and cand.shape[1] <= 128:
+        from .ivf import prune
+
+        return prune(x, cand, R, alpha, rows).long()
     n, K = cand.shape
     batch = max(64, min(batch, int(1.5e9 // (K * K * 4 + K * x.shape[1] * 4))))
     out = torch.full((n, R), -1, dtype=torch.long, device=x.device)
@@ -249,7 +256,7 @@ def vamana_pass(x: torch.Tensor, g: torch.Tensor, start: int, R: int, L: int, al
         V = _f32(x[cand.clamp_min(0)])
         d = ((V - _f32(x[p])[:, None, :]) ** 2).sum(-1)
         cand, d = _dedupe_sorted(cand, d)
-        g[p] = robust_prune(x, cand, d, R, alpha)
+        g[p] = robust_prune(x, cand, d, R, alpha, rows=p)
         g = _offer_reverse(x, g, p, R, alpha)
     return g
 
@@ -294,7 +301,7 @@ def _offer_reverse(x: torch.Tensor, g: torch.Tensor, p: torch.Tensor, R: int, al
         rows[small] = cand[small, :R]
         if bool((~small).any()):
             big = torch.nonzero(~small).squeeze(1)
-            rows[big] = robust_prune(x, cand[big], d[big], R, alpha)
+            rows[big] = robust_prune(x, cand[big], d[big], R, alpha, rows=u[big])
         g[u] = rows
     return g
 
@@ -314,7 +321,7 @@ def build(x: torch.Tensor, R: int, alpha: float = 1.2, K: int | None = None, n_c
     med = medoid(x)
     cand, cand_d = knn_candidates(x, K, n_coarse=n_coarse, nprobe=nprobe, seed=seed)
     r_loc = max(1, R - random_edges) if n > R + 1 else R
-    g = robust_prune(x, cand, cand_d, r_loc, alpha)
+    g = robust_prune(x, cand, cand_d, r_loc, alpha, rows=torch.arange(n, device=x.device))
     if r_loc < R:
         gen = torch.Generator(device="cpu")
         gen.manual_seed(seed + 101)

@@ -76,6 +76,50 @@ def write_disk_index(path: str, data: np.ndarray, graph: np.ndarray, degrees: np
     return {"n": n, "dim": dim, "node_len": nl, "npp": npp, "num_pages": num_pages, "R": R}
 
 
+def write_disk_index_torch(path: str, x, graph, degrees, medoid: int, R: int, chunk_nodes: int = 1 << 20) -> dict:
+    """write_disk_index for tensors on the GPU: every chunk of pages is laid
+    out on the device (vector, degree, neighbour slots, zero padding) and
+    written as it is copied back, so no host copy of the whole base is made.
+    ``graph`` rows hold their neighbours first (``degrees`` of them)."""
+    import torch
+
+    n, dim = x.shape
+    if x.dtype not in (torch.uint8, torch.float32):
+        raise ValueError("data must be uint8 or float32")
+    elt = x.element_size()
+    nl = node_len(dim, elt, R)
+    npp = PAGE // nl
+    if npp < 1:
+        raise ValueError("a node does not fit one 4 KB page")
+    num_pages = (n + npp - 1) // npp
+    file_size = PAGE * (num_pages + 1)
+    meta = np.array([n, dim, medoid, nl, npp, 0, 0, 0, file_size], dtype=np.uint64)
+    header = np.zeros(PAGE, dtype=np.uint8)
+    hb = struct.pack("<II", len(meta), 1) + meta.tobytes()
+    header[: len(hb)] = np.frombuffer(hb, dtype=np.uint8)
+    dev = x.device
+    cols = torch.arange(R, device=dev)
+    with open(path, "wb") as f:
+        f.write(header.tobytes())
+        step = max(npp, (chunk_nodes // npp) * npp)
+        for s in range(0, n, step):
+            e = min(n, s + step)
+            cnt = e - s
+            pages = (cnt + npp - 1) // npp
+            rec = torch.zeros((pages * npp, nl), dtype=torch.uint8, device=dev)
+            rec[:cnt, : dim * elt] = x[s:e].contiguous().view(torch.uint8).view(cnt, dim * elt)
+            deg = degrees[s:e].to(device=dev, dtype=torch.int32)
+            adj = torch.zeros((cnt, R + 1), dtype=torch.int32, device=dev)
+            adj[:, 0] = deg
+            adj[:, 1:] = torch.where(cols[None, :] < deg[:, None], graph[s:e, :R].to(device=dev, dtype=torch.int32),
+                                     torch.zeros((), dtype=torch.int32, device=dev))
+            rec[:cnt, dim * elt:] = adj.view(torch.uint8).view(cnt, (R + 1) * 4)
+            pg = torch.zeros((pages, PAGE), dtype=torch.uint8, device=dev)
+            pg[:, : npp * nl] = rec.view(pages, npp * nl)
+            f.write(pg.cpu().numpy())
+    return {"n": n, "dim": dim, "node_len": nl, "npp": npp, "num_pages": num_pages, "R": R}
+
+
 def _bin_block(arr: np.ndarray) -> bytes:
     rows, cols = arr.shape
     return struct.pack("<ii", rows, cols) + np.ascontiguousarray(arr).tobytes()
@@ -124,14 +168,17 @@ def write_nav(directory: str, data: np.ndarray, graph: np.ndarray, degrees: np.n
         f.write("\n".join(str(int(x)) for x in mapping) + "\n")
     degrees = np.asarray(degrees, dtype=np.int64)
     max_deg = int(degrees.max()) if n else 0
-    body = bytearray()
-    for i in range(n):
-        d = int(degrees[i])
-        body += struct.pack("<I", d) + np.asarray(graph[i, :d], dtype=np.uint32).tobytes()
-    size = 24 + len(body)
+    graph = np.asarray(graph)
+    starts = np.cumsum(degrees + 1) - (degrees + 1)
+    body = np.empty(int((degrees + 1).sum()), dtype=np.uint32)
+    body[starts] = degrees
+    cols = np.arange(graph.shape[1] if graph.ndim == 2 else 0)
+    mask = cols[None, :] < degrees[:, None]
+    body[(starts[:, None] + 1 + cols[None, :])[mask]] = graph[mask].astype(np.uint32)
+    size = 24 + body.nbytes
     with open(os.path.join(directory, "nav_index"), "wb") as f:
         f.write(struct.pack("<QIIQ", size, max_deg, start, 0))
-        f.write(bytes(body))
+        f.write(body.tobytes())
 
 
 @dataclass

@@ -57,9 +57,13 @@ enum {
   GANN_PREC_BF16_CC = 3  /* BF16 tables built per query on CUDA cores (FP32 then rounded) */
 };
 
-/* options of gann_search_batch; zero-initialised = defaults */
+/* options of gann_search_batch; zero-initialised = defaults, except that a
+ * zero precision is GANN_PREC_FP32. Passing opts = NULL selects
+ * GANN_PREC_BF16X3: the split-BF16 tensor-core tables, whose error against
+ * FP64 stays within BF16 storage rounding (single-pass GANN_PREC_BF16 loses
+ * up to 2^-5 of a chunk's range to cancellation in |r|^2 - 2 r.P + |P|^2). */
 typedef struct {
-  int32_t precision;   /* GANN_PREC_*; default GANN_PREC_BF16 */
+  int32_t precision;   /* GANN_PREC_*; opts = NULL means GANN_PREC_BF16X3 */
   int32_t beam_width;  /* warps (nodes expanded per step) per query: 1, 2, 4 or 8; 0 = 4 */
   int32_t hash_bits;   /* visited cache of 2^hash_bits ids per query; 0 = sized from L */
   int32_t reserved[5];
@@ -195,11 +199,16 @@ int gann_search_device_ex(gann_t* h, const float* d_queries, int nq, int topk, i
  * whole call; no per-query counters. The call allocates nothing: its scratch
  * (work counter, BF16 tables) is a fixed 8 MiB + 256 B array inside the
  * library, held on every GPU that loads libgann until the process exits.
- * Limits: nq <= 512 per call and, for tensor-core tables, at most 32 PQ
- * chunks; larger requests return GANN_ERANGE. All calls on a device share the
- * array: calls whose work overlaps on the GPU race on it and must be
- * serialised by the caller. The first call on a device looks up the array's
- * device address; make it before any stream capture.
+ * Options left 0 (or opts NULL) take the same defaults as
+ * gann_search_batch_device, the handle's gann_autotune choices included.
+ * Limits, tensor-core tables (GANN_PREC_BF16, GANN_PREC_BF16X3) only: nq <= 512
+ * per call and at most 32 PQ chunks; larger requests return GANN_ERANGE. The
+ * FP32 and CUDA-core BF16 precisions use only the work counter and take any nq.
+ * All calls on a device share the array: calls whose work overlaps on the GPU
+ * race on it and must be serialised by the caller. Each call looks up the
+ * array's device address in the current context (no allocation); the first
+ * call on a device may load the library's device code, so make it before any
+ * stream capture.
  */
 int gann_search_batch_noalloc(gann_t* h, const float* d_queries, int nq, int topk, int ef_search,
                               const gann_batch_opts_t* opts, int32_t* d_nns, float* d_distances,
@@ -300,6 +309,19 @@ int gann_set_fma(gann_t* h, int fma_table, int fma_exact);
  * std::shuffle and std::mt19937(seed), the first num_samp kept and sorted.
  * Replaces bin/gen_small_file.cpp:12-25 (seed 114514 there). */
 int gann_sample_pivots(int64_t num_data, int64_t num_samp, uint32_t seed, int32_t* out);
+
+/* RobustPrune for the index builder (index preparation, device buffers): for
+ * each of n_rows points (d_rows[r], or r when d_rows is NULL) keep at most R of
+ * its K candidate ids (d_cand, n_rows x K, -1 = none; the point itself,
+ * repeats and ids outside [0, n) are ignored) in order of squared L2 distance,
+ * dropping every candidate c that a kept neighbour j occludes:
+ * alpha * d(j, c) < d(p, c). d_x is n x dim uint8 or float32 (dtype); d_out
+ * is n_rows x R, -1 padded. Enqueued on `stream`. Replaces the pruning step of
+ * DiskANN's Vamana build, which the reference calls through
+ * scripts/build_diskann_index.sh:7 (DiskANN is an empty submodule there). */
+int gann_build_prune(const void* d_x, int dtype, int64_t n, int dim, const int32_t* d_rows,
+                     const int32_t* d_cand, int64_t n_rows, int K, int R, float alpha, int32_t* d_out,
+                     void* stream);
 
 /* Message for the last failing call on this thread. */
 const char* gann_last_error(void);

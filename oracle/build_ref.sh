@@ -14,9 +14,13 @@
 #    assert().
 #  * Device code keeps nvcc's defaults (-fmad=true), like the reference build.
 #
-# Usage: oracle/build_ref.sh [reference_dir]   (default /root/reference)
+# Usage: oracle/build_ref.sh <reference_dir>   (or $GANN_REF_DIR)
 set -euo pipefail
-REF=${1:-${GANN_REF_DIR:-/root/reference}}
+REF=${1:-${GANN_REF_DIR:-}}
+if [ -z "$REF" ]; then
+  echo "usage: build_ref.sh <reference_dir> (or set GANN_REF_DIR)" >&2
+  exit 2
+fi
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT="$HERE/_ref"
 OBJ="$OUT/obj"

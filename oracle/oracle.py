@@ -140,11 +140,22 @@ def max_threads() -> int:
 
 class Reference:
     """The reference's own search path built from its sources (oracle/build_ref.sh).
-    Needs a GPU; used only to pin the oracle and the product."""
+    Needs a GPU; used only to pin the oracle and the product.
 
-    def __init__(self, index_file: str, pq_prefix: str, nav_dir: str | None, dtype: int):
+    Every call is screened by the oracle first: the reference kernel is given
+    only the queries for which the oracle's walk stays out of the regimes where
+    the reference is undefined (FLAG_REF_UNDEFINED and the other flags: a list
+    that exhausts below L makes src/impl/pure_mem.cuh:380-419 expand a sentinel
+    id and read outside the index, which faulted the GPU once). ``screen_fma``
+    lists the (table, exact) FMA settings the screen runs under; a query
+    flagged under any of them is skipped. The reference build's own setting,
+    settled black-box on the committed fixtures, is (1, 1)."""
+
+    def __init__(self, index_file: str, pq_prefix: str, nav_dir: str | None, dtype: int,
+                 screen_fma=((1, 1),)):
         if not REF_LIB.exists():
             raise FileNotFoundError(f"{REF_LIB} not built")
+        self.screens = [Oracle(index_file, pq_prefix, nav_dir, dtype, bool(ft), bool(fe)) for ft, fe in screen_fma]
         L = ctypes.CDLL(str(REF_LIB))
         L.gref_open.restype = _P
         L.gref_open.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, _I]
@@ -155,20 +166,46 @@ class Reference:
         self.h = L.gref_open(index_file.encode(), pq_prefix.encode(), (nav_dir or "").encode(), dtype)
         if not self.h:
             raise RuntimeError("reference init_pure_mem failed")
+        self._screened = {}
+        self.last_skipped = 0
 
-    def search(self, q: np.ndarray, k: int, L: int):
+    def screen(self, q: np.ndarray, k: int, L: int, threads: int = 0) -> np.ndarray:
+        """Indices of the rows of q that every screen passes (flags == 0)."""
+        import hashlib
+
         q = np.ascontiguousarray(q, dtype=np.float32)
-        nq = q.shape[0]
+        key = (hashlib.sha1(q.tobytes()).hexdigest(), q.shape, k, L)
+        if key not in self._screened:
+            ok = np.ones(q.shape[0], bool)
+            for o in self.screens:
+                *_, flags, _ = o.search(q, k, L, threads=threads)
+                ok &= flags == 0
+            self._screened = {key: np.nonzero(ok)[0]}
+        return self._screened[key]
+
+    def search(self, q: np.ndarray, k: int, L: int, threads: int = 0):
+        """Runs the reference on the screened rows of q. Returns (rows, ids,
+        dists, found, seconds): rows are the indices into q that ran, the
+        outputs hold one row per entry of rows."""
+        q = np.ascontiguousarray(q, dtype=np.float32)
+        rows = self.screen(q, k, L, threads)
+        self.last_skipped = int(q.shape[0] - rows.size)
+        qs = np.ascontiguousarray(q[rows])
+        nq = qs.shape[0]
         ids = np.zeros((nq, k), np.int32)
         dis = np.zeros((nq, k), np.float32)
         fnd = np.zeros(nq, np.int32)
         t = ctypes.c_double(0.0)
-        rc = self.L.gref_search(self.h, _p(q), nq, k, L, _p(ids), _p(dis), _p(fnd), ctypes.byref(t))
-        if rc:
-            raise RuntimeError("reference search failed")
-        return ids, dis, fnd, t.value
+        if nq:
+            rc = self.L.gref_search(self.h, _p(qs), nq, k, L, _p(ids), _p(dis), _p(fnd), ctypes.byref(t))
+            if rc:
+                raise RuntimeError("reference search failed")
+        return rows, ids, dis, fnd, t.value
 
     def close(self):
         if self.h:
             self.L.gref_close(self.h)
             self.h = None
+        for o in self.screens:
+            o.close()
+        self.screens = []

@@ -8,8 +8,14 @@ contraction sites (src/impl/pq.cuh:40, src/impl/util.cuh:37): the oracle is run
 with the four switch settings and the one whose outputs equal the reference's
 is recorded (``fma_table``, ``fma_exact``) with the per-setting mismatch counts.
 
-    python tests/golden/make_ref_golden.py gpurun_out/golden
+    python tests/golden/make_ref_golden.py <out_dir>
 Copy the resulting ref.npz files next to the fixtures to commit them.
+
+The reference kernel only ever sees queries that the oracle, under each of the
+four FMA settings, runs without an undefined-regime flag (oracle.Reference
+screens every call); the fixtures' cases have none, and the script fails if
+any query is screened out, since a fixture row without a reference output
+could not be pinned.
 """
 from __future__ import annotations
 
@@ -35,10 +41,13 @@ def main(out_dir: str) -> int:
         with tempfile.TemporaryDirectory() as tmp:
             meta = unpack(name, Path(tmp))
             q = meta["queries"]
-            ref = Reference(meta["index_file"], meta["pq_prefix"], meta["nav_dir"], meta["dtype"])
+            ref = Reference(meta["index_file"], meta["pq_prefix"], meta["nav_dir"], meta["dtype"],
+                            screen_fma=((1, 1), (1, 0), (0, 1), (0, 0)))
             res = {}
             for k, L in meta["cases"]:
-                ids, dis, fnd, secs = ref.search(q, k, L)
+                rows, ids, dis, fnd, secs = ref.search(q, k, L)
+                if rows.size != q.shape[0]:
+                    raise SystemExit(f"{name} k={k} L={L}: {q.shape[0] - rows.size} queries flagged by the oracle")
                 res[f"ids_k{k}_L{L}"], res[f"dists_k{k}_L{L}"], res[f"found_k{k}_L{L}"] = ids, dis, fnd
             ref.close()
             mism = {}
@@ -66,4 +75,6 @@ def main(out_dir: str) -> int:
 
 
 if __name__ == "__main__":
-    sys.exit(main(sys.argv[1] if len(sys.argv) > 1 else "gpurun_out/golden"))
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: make_ref_golden.py <out_dir>")
+    sys.exit(main(sys.argv[1]))

@@ -69,41 +69,47 @@ def test_wait_for_times_out(tmp_path):
 
 
 def test_calibrate_finds_smallest_L():
-    """calibrate(): walk the L ladder, then bisect to a step of 8, returning the
-    smallest L whose recall reaches the target (host logic, fake runner)."""
-    import sys
-    import types
-
-    import numpy as np
-
+    """calibrate_L(): walk the L ladder, then bisect to a step of 8, returning
+    the smallest L whose recall reaches the target (host logic; both arms use
+    it, so bit-exact forms land on the same L)."""
     sys.path.insert(0, str(ROOT))
     import bench
-
-    class FakeG:
-        def check(self, stream=None):
-            pass
 
     for threshold in (37, 200, 384, 393, 1000):
         calls = []
 
-        class Runner:
-            g = FakeG()
+        def recall_for(L):
+            calls.append(L)
+            return 0.96 if L >= threshold else 0.5
 
-            def run(self, L, counters=False):
-                calls.append(L)
-                # recall >= 0.95 exactly when L >= threshold
-                self.ids = types.SimpleNamespace(cpu=lambda L=L: types.SimpleNamespace(numpy=lambda: L))
-
-        orig = bench.recall_at
-        bench.recall_at = lambda ids, gt, k: 0.96 if ids >= threshold else 0.5
-        try:
-            import torch
-
-            sync = torch.cuda.synchronize
-            torch.cuda.synchronize = lambda: None
-            L, rec = bench.calibrate(Runner(), None, 10, 0.95)
-        finally:
-            bench.recall_at = orig
-            torch.cuda.synchronize = sync
+        L, rec = bench.calibrate_L(recall_for, 10, 0.95)
         assert rec >= 0.95 and L >= threshold and L - threshold < 8, (threshold, L, calls)
         assert L % 8 == 0 or L in bench.L_LADDER
+
+
+def test_recall_measures_match_the_tooling():
+    """bench.py's vectorised calc_recall / recall_unique equal the indexing
+    package's loops (bin/utils.hpp:105-117 and its unique-id variant)."""
+    import numpy as np
+
+    sys.path.insert(0, str(ROOT))
+    import bench
+    from gustann_b200.indexing import groundtruth
+
+    rng = np.random.default_rng(5)
+    gt = rng.integers(0, 50, size=(40, 100)).astype(np.int32)
+    ids = rng.integers(0, 50, size=(40, 10)).astype(np.int32)
+    ids[:, 3] = ids[:, 2]  # repeated ids count twice in calc_recall, once in recall_unique
+    for k in (1, 5, 10):
+        assert bench.calc_recall(ids, gt, k) == groundtruth.recall(ids, gt, k)
+        assert bench.recall_unique(ids, gt, k) == groundtruth.recall_unique(ids, gt, k)
+
+
+def test_both_arms_state_the_same_config():
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    meta = {"workload": "c2", "n": 100_000_000, "dim": 128, "kind": "u8", "R": 32, "M": 32, "nav": 1_000_000}
+    a = bench.config_of(meta, 10_000, 10)
+    b = bench.config_of(dict(meta), 10_000, 10)
+    assert a == b and a["workload"] == "c2" and "l2" in a and a["queries_per_step"] == 10_000

@@ -81,3 +81,75 @@ def test_small_build_is_valid_and_searchable(tmp_path, oracle_mod):
     ids, dis, fnd, hops, flags, ent = o.search(qs.astype(np.float32), 10, 64)
     assert not flags.any()
     assert groundtruth.recall(ids, gt, 10) > 0.9
+
+
+def test_partitioned_build_is_valid_and_searchable(tmp_path, oracle_mod):
+    """The large-index builder (ivf: leaf k-NN, RobustPrune, reverse edges,
+    the pivot graph embedded as long edges) on a small mixture, on the CPU:
+    valid rows, pivot-graph edges present in the sampled points' rows, and the
+    oracle reaches high recall over its files."""
+    from gustann_b200 import sample_pivots
+    from gustann_b200.indexing import ivf
+
+    base, qs = synth.make("u8", 6000, 32, 12, 60, backend="numpy")
+    f = build_index(base, str(tmp_path), R=16, M=8, nav_samples=300, method="ivf", leaf=512)
+    di = formats.read_disk_index(f.index_file, np.uint8)
+    np.testing.assert_array_equal(di.data, base)
+    assert di.degrees.min() >= 1 and di.degrees.max() <= 16
+    for u in range(0, 6000, 7):
+        nb = di.graph[u, :di.degrees[u]]
+        assert np.all((nb >= 0) & (nb < 6000)) and u not in nb and len(set(nb.tolist())) == len(nb)
+    piv = sample_pivots(6000, 300)
+    nav = formats.read_nav(f.nav_dir) if hasattr(formats, "read_nav") else None
+    # every sampled point keeps some of its pivot-graph neighbours as long edges
+    pset = set(piv.tolist())
+    frac = np.mean([any(int(v) in pset for v in di.graph[u, :di.degrees[u]]) for u in piv])
+    assert frac > 0.9
+    assert builder.reachable_from(di.graph, di.degrees, di.medoid).mean() > 0.99
+    gt = groundtruth.knn(torch.from_numpy(base), torch.from_numpy(qs), 10)
+    o = oracle_mod.Oracle(f.index_file, f.pq_prefix, f.nav_dir, 0)
+    ids, dis, fnd, hops, flags, ent = o.search(qs.astype(np.float32), 10, 64)
+    assert not flags.any()
+    assert groundtruth.recall(ids, gt, 10) > 0.9
+    del nav, ivf
+
+
+def test_leaf_candidates_are_the_exact_neighbours_inside_well_separated_leaves():
+    from gustann_b200.indexing import ivf
+
+    base, _ = synth.make("u8", 5000, 32, 5, 1, backend="numpy")
+    x = torch.from_numpy(base)
+    cand = ivf.leaf_candidates(x, 16, 1000, 3)
+    d = builder.sqdist(x[:300], x)
+    d[torch.arange(300), torch.arange(300)] = float("inf")
+    exact = torch.topk(d, 16, largest=False).indices
+    hit = np.mean([len(set(cand[i].tolist()) & set(exact[i].tolist())) / 16 for i in range(300)])
+    assert hit > 0.97
+    assert (cand[torch.arange(5000), 0] != torch.arange(5000)).all()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["u8", "f32"])
+def test_prune_kernel_follows_the_rule(kind):
+    """gann_build_prune (one warp per point) against builder.robust_prune on
+    the same candidate rows (sorted by distance then id, repeats and the point
+    itself dropped): identical rows for uint8 (exact int32 distances), nearly
+    identical for float (FP32 sums in another order)."""
+    from gustann_b200.indexing import ivf
+
+    rng = np.random.default_rng(4)
+    n, dim, K, R, alpha = 3000, 128 if kind == "u8" else 96, 96, 24, 1.2
+    if kind == "u8":
+        x = torch.from_numpy(rng.integers(0, 256, size=(n, dim), dtype=np.uint8))
+    else:
+        x = torch.from_numpy(rng.standard_normal((n, dim)).astype(np.float32))
+    cand = torch.from_numpy(rng.integers(-1, n, size=(n, K)).astype(np.int32))
+    cand[:50, 5] = torch.arange(50, dtype=torch.int32)  # the point itself
+    cand[:50, 7] = cand[:50, 6]                          # a repeated id
+    got = ivf.prune(x.cuda(), cand.cuda(), R, alpha).cpu()
+    want = ivf.prune(x, cand, R, alpha)
+    if kind == "u8":
+        assert torch.equal(got, want)
+    else:
+        same = (got == want).all(1).float().mean().item()
+        assert same > 0.98, same

@@ -17,19 +17,15 @@ import pytest
 import gustann_b200 as gb
 
 
-@pytest.mark.gpu
-@pytest.mark.parametrize("precision", [gb.PREC_BF16, gb.PREC_FP32])
-def test_noalloc_matches_batch_device_on_two_calls(golden, precision):
+def _two_calls(g, meta, precision, opts, beam_width, hash_bits):
+    """Two no-alloc calls in a row, the second on the first call's leftovers,
+    each compared with gann_search_batch_device on the same batch."""
     import torch
 
-    meta = golden["u8_nav"]
-    g = gb.GustANN(gb.DataType.UINT8)
-    g.init_pure_mem(gb.GustANNConfig(meta["index_file"], meta["pq_prefix"], meta["nav_dir"]))
     k, L = 10, 48
     stream = torch.cuda.current_stream().cuda_stream
-    opts = gb.GustANN._opts(precision, 4, 10)
     batches = [meta["queries"], np.ascontiguousarray(meta["queries"][:150][::-1])]
-    for q in batches:  # two calls in a row, the second on the first call's leftovers
+    for q in batches:
         nq = q.shape[0]
         dq = torch.from_numpy(q).cuda()
 
@@ -40,8 +36,10 @@ def test_noalloc_matches_batch_device_on_two_calls(golden, precision):
 
         ref, got = outs(), outs()
         g.search_batch_device(dq.data_ptr(), nq, 0, 0, k, L, ref[0].data_ptr(), ref[1].data_ptr(),
-                              ref[2].data_ptr(), precision=precision, beam_width=4, hash_bits=10, stream=stream)
-        rc = gb.lib().gann_search_batch_noalloc(g.handle, dq.data_ptr(), nq, k, L, ctypes.byref(opts),
+                              ref[2].data_ptr(), precision=precision, beam_width=beam_width, hash_bits=hash_bits,
+                              stream=stream)
+        rc = gb.lib().gann_search_batch_noalloc(g.handle, dq.data_ptr(), nq, k, L,
+                                                None if opts is None else ctypes.byref(opts),
                                                 got[0].data_ptr(), got[1].data_ptr(), got[2].data_ptr(),
                                                 gb._stream(stream))
         assert rc == gb.GANN_OK, gb.lib().gann_last_error()
@@ -50,6 +48,35 @@ def test_noalloc_matches_batch_device_on_two_calls(golden, precision):
         np.testing.assert_allclose(got[1].cpu().numpy(), ref[1].cpu().numpy(), rtol=0, atol=0)
         np.testing.assert_array_equal(got[2].cpu().numpy(), ref[2].cpu().numpy())
         assert (got[2].cpu().numpy() == k).all()
+
+
+def _open(meta):
+    g = gb.GustANN(gb.DataType.UINT8)
+    g.init_pure_mem(gb.GustANNConfig(meta["index_file"], meta["pq_prefix"], meta["nav_dir"]))
+    return g
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [gb.PREC_BF16, gb.PREC_BF16X3, gb.PREC_BF16_CC, gb.PREC_FP32])
+def test_noalloc_matches_batch_device_on_two_calls(golden, precision):
+    meta = golden["u8_nav"]
+    g = _open(meta)
+    _two_calls(g, meta, precision, gb.GustANN._opts(precision, 4, 10), 4, 10)
+    g.close()
+
+
+@pytest.mark.gpu
+def test_noalloc_defaults_follow_the_autotuned_handle(golden):
+    """opts NULL (and zeroed beam width / cache size) take the handle's tuned
+    defaults, as gann_search_batch_device does."""
+    import torch
+
+    meta = golden["u8_nav"]
+    g = _open(meta)
+    dq = torch.from_numpy(meta["queries"]).cuda()
+    g.autotune(dq.data_ptr(), dq.shape[0], 10, 48, gb.PREC_BF16)
+    _two_calls(g, meta, gb.PREC_BF16, None, 0, 0)
+    _two_calls(g, meta, gb.PREC_BF16, gb.GustANN._opts(gb.PREC_BF16, 0, 0), 0, 0)
     g.close()
 
 
@@ -69,4 +96,10 @@ def test_noalloc_rejects_more_than_its_scratch_holds(golden):
                                             out_d.data_ptr(), out_f.data_ptr(), None)
     assert rc == gb.GANN_ERANGE
     assert "512" in gb.lib().gann_last_error().decode()
+    # FP32 tables never touch the table region: any batch size is taken
+    opts = gb.GustANN._opts(gb.PREC_FP32, 4, 10)
+    rc = gb.lib().gann_search_batch_noalloc(g.handle, dq.data_ptr(), nq, 10, 48, ctypes.byref(opts),
+                                            out_i.data_ptr(), out_d.data_ptr(), out_f.data_ptr(), None)
+    assert rc == gb.GANN_OK, gb.lib().gann_last_error()
+    g.check()
     g.close()
