@@ -393,7 +393,13 @@ def serving_sweep(g, meta, rates, seconds, max_batch, streams):
     q = meta["queries"]
     ks = rng.choice(np.array([1, 10, 100], np.int32), len(q)).astype(np.int32)
     Ls = np.exp(rng.uniform(np.log(32), np.log(512), len(q))).astype(np.int32)
-    srv = gb.Server(g, max_batch=max_batch, streams=streams, topk_max=100, ef_max=512, precision=gb.PREC_BF16X3)
+    # admission budget: every request slot at a request of (k 10, L 256), so a
+    # pipeline full of long-list requests refuses them before short ones
+    probe = gb.Server(g, max_batch=max_batch, streams=streams, topk_max=100, ef_max=512, precision=gb.PREC_BF16X3)
+    budget_kib = max_batch * (streams + 1) * probe.request_bytes(10, 256) // 1024
+    probe.stop()
+    srv = gb.Server(g, max_batch=max_batch, streams=streams, topk_max=100, ef_max=512, precision=gb.PREC_BF16X3,
+                    mem_budget_kib=budget_kib)
     out = []
     try:
         srv.open_loop(q, rates[0], 0.2, topk=ks, ef_search=Ls, seed=99)  # warm-up
@@ -406,7 +412,9 @@ def serving_sweep(g, meta, rates, seconds, max_batch, streams):
     finally:
         srv.stop()
     return {"k": [1, 10, 100], "L": "log-uniform [32, 512]", "max_batch": max_batch, "streams": streams,
-            "seconds_per_rate": seconds, "precision": "bf16x3", "points": out}
+            "seconds_per_rate": seconds, "precision": "bf16x3", "mem_budget_kib": budget_kib,
+            "admission": "by bytes: each request charged its own list, visited cache, table, query and result row",
+            "points": out}
 
 
 def cpu_baseline(meta, L, k, budget_s=15.0):

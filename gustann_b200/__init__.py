@@ -71,7 +71,7 @@ class ServerOpts(ctypes.Structure):
     _fields_ = [("max_batch", ctypes.c_int32), ("streams", ctypes.c_int32), ("topk_max", ctypes.c_int32),
                 ("ef_max", ctypes.c_int32), ("precision", ctypes.c_int32), ("beam_width", ctypes.c_int32),
                 ("hash_bits", ctypes.c_int32), ("max_wait_us", ctypes.c_int32), ("min_batch", ctypes.c_int32),
-                ("reserved", ctypes.c_int32 * 7)]
+                ("mem_budget_kib", ctypes.c_int32), ("reserved", ctypes.c_int32 * 6)]
 
 
 class LoadStats(ctypes.Structure):
@@ -113,6 +113,7 @@ _SIGNATURES = {
     "gann_autotune": (_I, [_P, _P, _I, _I, _I, _I, _P, ctypes.POINTER(ctypes.c_double)]),
     "gann_server_start": (_I, [_P, ctypes.POINTER(ServerOpts), ctypes.POINTER(_P)]),
     "gann_server_submit": (_I, [_P, _P, _I, _I, ctypes.c_uint64]),
+    "gann_server_request_bytes": (ctypes.c_int64, [_P, _I, _I]),
     "gann_server_poll": (_I, [_P, _I, _P, _P, _P, _P, _P, ctypes.POINTER(_I)]),
     "gann_server_stop": (_I, [_P]),
     "gann_server_open_loop": (_I, [_P, _P, _I, _P, _P, ctypes.c_double, ctypes.c_double, ctypes.c_uint64,
@@ -360,17 +361,21 @@ class Server:
     """Continuous-batching server over one open index (gann_server_*)."""
 
     def __init__(self, index: GustANN, max_batch: int = 1024, streams: int = 4, topk_max: int = 100,
-                 ef_max: int = 512, precision: int = PREC_BF16, beam_width: int = 0, hash_bits: int = 0,
-                 max_wait_us: int = 100, min_batch: int = 0):
+                 ef_max: int = 512, precision: int = PREC_BF16X3, beam_width: int = 0, hash_bits: int = 0,
+                 max_wait_us: int = 100, min_batch: int = 0, mem_budget_kib: int = 0):
         self.index = index
         self.dim = index.info()["dim"]
         o = ServerOpts()
         (o.max_batch, o.streams, o.topk_max, o.ef_max, o.precision, o.beam_width, o.hash_bits, o.max_wait_us,
-         o.min_batch) = (max_batch, streams, topk_max, ef_max, precision, beam_width, hash_bits, max_wait_us,
-                         min_batch)
+         o.min_batch, o.mem_budget_kib) = (max_batch, streams, topk_max, ef_max, precision, beam_width, hash_bits,
+                                           max_wait_us, min_batch, mem_budget_kib)
         self.topk_max = topk_max
         self._s = _P()
         _check(lib().gann_server_start(index.handle, ctypes.byref(o), ctypes.byref(self._s)))
+
+    def request_bytes(self, topk: int, ef_search: int) -> int:
+        """The admission charge of one request (gann_server_request_bytes)."""
+        return int(lib().gann_server_request_bytes(self._s, topk, ef_search))
 
     def submit(self, query: np.ndarray, topk: int, ef_search: int, tag: int) -> bool:
         """False when the server's request budget is full (GANN_EBUSY)."""

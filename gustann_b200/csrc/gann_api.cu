@@ -490,7 +490,8 @@ int enqueue_batch(gann_t* h, const float* d_q, int nq, const int32_t* d_k, const
       h->cap_tables = need;
     }
     __nv_bfloat16* tab = tables ? tables : h->d_tables;
-    e = gann::launch_table_tc(h->dx, (int)h->hx.dim, h->hx.pq_m, d_q, nq, prec == GANN_PREC_BF16X3, tab, s, nq_dev);
+    e = gann::launch_table_tc(h->dx, (int)h->hx.dim, h->hx.pq_m, d_q, nq, prec == GANN_PREC_BF16X3, tab, s,
+                                h->num_sms, nq_dev);
     if (e != cudaSuccess) return set_error(GANN_ECUDA, std::string("table build: ") + cudaGetErrorString(e));
     p.tables = tab;
   }
@@ -615,7 +616,8 @@ int gann_pq_tables(gann_t* h, const float* queries, int nq, int precision, float
     else if (precision == GANN_PREC_BF16_CC)
       e = gann::launch_table_cc(h->dx, (int)h->hx.dim, h->hx.pq_m, dq, nq, h->fma_table, true, db, s);
     else
-      e = gann::launch_table_tc(h->dx, (int)h->hx.dim, h->hx.pq_m, dq, nq, precision == GANN_PREC_BF16X3, db, s);
+      e = gann::launch_table_tc(h->dx, (int)h->hx.dim, h->hx.pq_m, dq, nq, precision == GANN_PREC_BF16X3, db, s,
+                                  h->num_sms);
   }
   if (e == cudaSuccess && db) e = gann::widen_bf16(db, dt, tn, s);
   unsigned int err = 0;

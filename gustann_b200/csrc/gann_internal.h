@@ -180,7 +180,7 @@ size_t table_tc_smem(int M, int groups);
 // BF16 PQ tables of a query batch on the tensor cores (table_tc.cu):
 // tables[q][c][j] = |r_qc|^2 - 2 r_qc . P_cj + |P_cj|^2 with r = q - centroid.
 cudaError_t launch_table_tc(const DeviceIndex& ix, int dim, int M, const float* queries, int nq, int split3,
-                            __nv_bfloat16* tables, cudaStream_t stream, const int* nq_dev = nullptr);
+                            __nv_bfloat16* tables, cudaStream_t stream, int num_sms, const int* nq_dev = nullptr);
 
 // Per-warp shared-memory footprint of the plain kernel, in bytes.
 size_t plain_smem_per_warp(int M, int L, int max_m, int k, int dim);

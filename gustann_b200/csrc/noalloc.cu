@@ -89,7 +89,8 @@ extern "C" int gann_search_batch_noalloc(gann_t* h, const float* d_queries, int 
   __nv_bfloat16* tables = reinterpret_cast<__nv_bfloat16*>(static_cast<uint8_t*>(base) + kNoAllocHeader);
   if (e == cudaSuccess) e = cudaMemsetAsync(counter, 0, sizeof(int), s);  // the previous call left its count
   if (e == cudaSuccess && tc)
-    e = launch_table_tc(h->dx, (int)h->hx.dim, h->hx.pq_m, d_queries, nq, prec == GANN_PREC_BF16X3, tables, s);
+    e = launch_table_tc(h->dx, (int)h->hx.dim, h->hx.pq_m, d_queries, nq, prec == GANN_PREC_BF16X3, tables, s,
+                         h->num_sms);
   if (e == cudaSuccess) {
     BatchParams p{};
     p.ix = h->dx;

@@ -10,9 +10,12 @@
 // captured over them at start (gann_batch_graph_create: counter reset, table
 // build, persistent walk reading the batch size from device memory), so a
 // batch is its input copies, one graph launch and its output copies. Admission
-// is by that budget: a submit is refused (GANN_EBUSY) while every request slot
-// of the server is taken. Per-query state (candidate list, visited cache,
-// table) lives on the device for the life of its batch. A request's result
+// is by memory: each request is charged the device state its own L and k need
+// (candidate list, visited cache, table, query, result row; request_bytes),
+// and a submit is refused (GANN_EBUSY) when the requests held by the server --
+// waiting, on the GPU, or finished and not yet polled -- would exceed the byte
+// budget, or would take more request slots than the server has. Per-query
+// state lives on the device for the life of its batch. A request's result
 // depends only on the query, its k and L, and the server's options, not on
 // the other requests in its batch.
 #include <algorithm>
@@ -49,6 +52,7 @@ struct Slot {
   gann_batch_graph_t* graph = nullptr;
   std::vector<uint64_t> tags;
   std::vector<double> t_submit;
+  std::vector<int64_t> cost;
   int count = 0;
   bool busy = false;
 };
@@ -66,13 +70,17 @@ struct gann_server {
   std::vector<int32_t> rk, rl;
   std::vector<uint64_t> rtag;
   std::vector<double> rt;
+  std::vector<int64_t> rcost;
   int in_flight = 0;  // requests inside busy slots
+  int64_t budget = 0;      // admission budget in bytes
+  int64_t bytes_held = 0;  // charge of the waiting + running + unpolled requests
   // completions (ring of the same capacity; counted against the budget until polled)
   int dhead = 0, dsize = 0;
   std::vector<uint64_t> dtag;
   std::vector<int32_t> dfound, dids;
   std::vector<float> ddist;
   std::vector<double> dlat;
+  std::vector<int64_t> dcost;
   std::mutex mu;
   std::thread th;
   std::atomic<bool> stop{false};
@@ -114,7 +122,19 @@ cudaError_t alloc_slot(Slot& s, int B, int dim, int kmax) {
   if (e == cudaSuccess) e = cudaMalloc(&s.d_nq, sizeof(int32_t));
   s.tags.resize(B);
   s.t_submit.resize(B);
+  s.cost.resize(B);
   return e;
+}
+
+// Device state a request of (k, L) holds while the server has it: the sorted
+// candidate list (id + distance per entry), the visited cache (one id per
+// slot, sized from L as the batched form sizes it), the PQ table (BF16 or
+// FP32 per precision), the query and the result row (id + distance per k,
+// plus the found count).
+int64_t request_bytes(const gann_server* sv, int k, int L) {
+  const int tab = sv->o.precision == GANN_PREC_FP32 ? 4 : 2;
+  const int hb = sv->o.hash_bits ? sv->o.hash_bits : gann::batch_hash_bits(L);
+  return 8ll * L + 4ll * (1ll << hb) + (int64_t)tab * sv->M * gann::kPivots + 4ll * sv->dim + 8ll * k + 4;
 }
 
 // Publish a finished batch into the completion ring. Dispatcher thread only.
@@ -132,6 +152,7 @@ void complete(gann_server* sv, Slot& s, cudaError_t q) {
   for (int i = 0; i < s.count; i++) {
     const int r = (base + i) % sv->cap;
     sv->dtag[r] = s.tags[i];
+    sv->dcost[r] = s.cost[i];
     sv->dfound[r] = s.h_f[i];
     sv->dlat[r] = t - s.t_submit[i];
     std::memcpy(&sv->dids[(size_t)r * kmax], s.h_nns + (size_t)i * kmax, sizeof(int32_t) * kmax);
@@ -177,6 +198,7 @@ bool launch(gann_server* sv) {
     s->h_l[i] = sv->rl[r];
     s->tags[i] = sv->rtag[r];
     s->t_submit[i] = sv->rt[r];
+    s->cost[i] = sv->rcost[r];
   }
   {
     std::lock_guard<std::mutex> lk(sv->mu);
@@ -242,9 +264,13 @@ void dispatcher(gann_server* sv) {
 // Queue one request that arrived at time t. Caller holds mu.
 int submit_locked(gann_server* sv, const float* query, int topk, int ef_search, uint64_t tag, double t) {
   if (sv->error) return gann_internal_set_error(sv->error, sv->error_msg.c_str());
-  // admission: waiting + on the GPU + finished but not yet polled, against the budget
-  if (sv->size + sv->in_flight + sv->dsize >= sv->cap) return GANN_EBUSY;
+  // admission: waiting + on the GPU + finished but not yet polled, against
+  // the byte budget and the request slots
+  const int64_t cost = request_bytes(sv, topk, ef_search);
+  if (sv->size + sv->in_flight + sv->dsize >= sv->cap || sv->bytes_held + cost > sv->budget) return GANN_EBUSY;
   const int r = sv->tail;
+  sv->rcost[r] = cost;
+  sv->bytes_held += cost;
   std::memcpy(sv->rq.data() + (size_t)r * sv->dim, query, sizeof(float) * sv->dim);
   sv->rk[r] = topk;
   sv->rl[r] = ef_search;
@@ -271,7 +297,7 @@ int gann_server_start(gann_t* h, const gann_server_opts_t* opts, gann_server_t**
   if (!o.max_wait_us) o.max_wait_us = 100;
   if (!opts) o.precision = GANN_PREC_BF16X3;
   if (o.max_batch < 1 || o.streams < 1 || o.streams > 64 || o.topk_max < 1 || o.ef_max < 1 || o.topk_max > 4096 ||
-      o.ef_max > 4096 || o.max_wait_us < 0)
+      o.ef_max > 4096 || o.max_wait_us < 0 || o.mem_budget_kib < 0)
     return gann_internal_set_error(GANN_EINVAL, "bad server options");
   auto* sv = new gann_server();
   sv->h = h;
@@ -284,6 +310,10 @@ int gann_server_start(gann_t* h, const gann_server_opts_t* opts, gann_server_t**
   sv->rl.resize(sv->cap);
   sv->rtag.resize(sv->cap);
   sv->rt.resize(sv->cap);
+  sv->rcost.resize(sv->cap);
+  sv->dcost.resize(sv->cap);
+  sv->budget = o.mem_budget_kib > 0 ? (int64_t)o.mem_budget_kib * 1024
+                                    : (int64_t)sv->cap * request_bytes(sv, o.topk_max, o.ef_max);
   sv->dtag.resize(sv->cap);
   sv->dfound.resize(sv->cap);
   sv->dlat.resize(sv->cap);
@@ -320,6 +350,11 @@ int gann_server_start(gann_t* h, const gann_server_opts_t* opts, gann_server_t**
   return GANN_OK;
 }
 
+int64_t gann_server_request_bytes(const gann_server_t* sv, int topk, int ef_search) {
+  if (!sv || topk < 1 || ef_search < 1) return -1;
+  return request_bytes(sv, topk, ef_search);
+}
+
 int gann_server_submit(gann_server_t* sv, const float* query, int topk, int ef_search, uint64_t tag) {
   if (!sv || !query) return gann_internal_set_error(GANN_EINVAL, "null argument");
   if (topk < 1 || topk > sv->o.topk_max || ef_search < 1 || ef_search > sv->o.ef_max)
@@ -342,6 +377,7 @@ int gann_server_poll(gann_server_t* sv, int max_results, uint64_t* tags, int32_t
     if (distances) std::memcpy(distances + (size_t)i * kmax, &sv->ddist[(size_t)r * kmax], sizeof(float) * kmax);
     if (found_cnt) found_cnt[i] = sv->dfound[r];
     if (latency) latency[i] = sv->dlat[r];
+    sv->bytes_held -= sv->dcost[r];
   }
   sv->dhead = (sv->dhead + n) % sv->cap;
   sv->dsize -= n;

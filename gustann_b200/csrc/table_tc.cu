@@ -21,8 +21,13 @@
 // One CTA of 128 threads handles 128 queries; thread t owns query row t (TMEM
 // lane t). One elected thread issues tcgen05.mma; completion is tracked by
 // tcgen05.commit on an mbarrier; the epilogue reads TMEM with tcgen05.ld,
-// adds the norms, rounds to BF16 and stores the rows. Every wait is bounded:
-// on expiry the kernel sets kErrWaitLimit, frees its TMEM and returns.
+// adds the norms, rounds to BF16 and stores the rows. The chunks of a CTA run
+// as a two-stage pipeline: two B tile buffers and two TMEM accumulators (512
+// columns), so while the epilogue drains chunk c, the MMAs of chunk c + 1 run
+// and the B tiles of chunk c + 2 are on their way. Two CTAs on one SM take
+// the tensor memory in turn (tcgen05.alloc waits until the columns are free).
+// Every wait is bounded: on expiry the kernel sets kErrWaitLimit, lets its
+// copies and MMAs land, frees its TMEM and returns.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -38,7 +43,7 @@ constexpr int kN = 256;             // centroids per chunk (MMA N)
 constexpr int kK = 16;              // MMA K for BF16
 constexpr int kATileBytes = kTile * kK * 2;  // 4 KB
 constexpr int kBTileBytes = kN * kK * 2;     // 8 KB
-constexpr uint32_t kTmemCols = 256;
+constexpr uint32_t kTmemCols = 512;  // two 256-column accumulators
 constexpr long long kSpinLimit = 1ll << 22;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -144,14 +149,14 @@ struct TcParams {
 
 __global__ void __launch_bounds__(kTile, 1) table_tc_kernel(TcParams p) {
   extern __shared__ __align__(1024) uint8_t smem[];
-  // [A_hi groups][A_lo groups][B_hi][B_lo][rn: M x 128 floats][bars][tmem slot]
+  // [A_hi groups][A_lo groups][B_hi x2][B_lo x2][rn: M x 128 floats][bars][tmem slot]
   uint8_t* a_hi = smem;
   uint8_t* a_lo = a_hi + (size_t)p.groups * kATileBytes;
-  uint8_t* b_hi = a_lo + (size_t)p.groups * kATileBytes;
-  uint8_t* b_lo = b_hi + kBTileBytes;
-  float* rn = reinterpret_cast<float*>(b_lo + kBTileBytes);
-  uint64_t* bars = reinterpret_cast<uint64_t*>(rn + (size_t)p.M * kTile);  // [0] B copy, [1] MMA done
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2);
+  uint8_t* b_hi = a_lo + (size_t)p.groups * kATileBytes;  // stage s at b_hi + s * kBTileBytes
+  uint8_t* b_lo = b_hi + 2 * kBTileBytes;
+  float* rn = reinterpret_cast<float*>(b_lo + 2 * kBTileBytes);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(rn + (size_t)p.M * kTile);  // [0,1] B copies, [2,3] MMAs done
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 4);
   const int tid = threadIdx.x, warp = tid >> 5;
   const int q0 = blockIdx.x * kTile;
   const int qi = q0 + tid;
@@ -164,6 +169,7 @@ __global__ void __launch_bounds__(kTile, 1) table_tc_kernel(TcParams p) {
   // chunk range of this CTA: whole groups, split over gridDim.y
   const int gpb = (p.groups + gridDim.y - 1) / gridDim.y;
   const int c_begin = min(p.M, (int)blockIdx.y * gpb * G), c_end = min(p.M, ((int)blockIdx.y + 1) * gpb * G);
+  const int nc = c_end - c_begin;
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
@@ -172,8 +178,7 @@ __global__ void __launch_bounds__(kTile, 1) table_tc_kernel(TcParams p) {
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   if (tid == 0) {
-    mbar_init(&bars[0], 1);
-    mbar_init(&bars[1], 1);
+    for (int b = 0; b < 4; b++) mbar_init(&bars[b], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   // A operand: residual r = q - mu of this thread's query, split BF16 hi/lo,
@@ -210,50 +215,69 @@ __global__ void __launch_bounds__(kTile, 1) table_tc_kernel(TcParams p) {
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
   const uint32_t b_bytes = kBTileBytes * (p.split3 ? 2u : 1u);
+  // Chunk i of this CTA (c_begin + i) uses B stage i & 1 and TMEM columns
+  // [256 (i & 1), + 256); both barriers of a stage complete once per use, so
+  // use u = i >> 1 waits on parity u & 1.
+  auto issue_copy = [&](int i) {
+    const int st = i & 1, c = c_begin + i;
+    mbar_expect_tx(&bars[st], b_bytes);
+    bulk_copy_g2s(b_hi + st * kBTileBytes, p.bpanel_hi + (size_t)c * kBTileBytes, kBTileBytes, &bars[st]);
+    if (p.split3)
+      bulk_copy_g2s(b_lo + st * kBTileBytes, p.bpanel_lo + (size_t)c * kBTileBytes, kBTileBytes, &bars[st]);
+  };
+  // tid 0 only: wait for chunk i's B tiles, then issue its MMAs
+  auto issue_mma = [&](int i) -> bool {
+    const int st = i & 1, c = c_begin + i;
+    if (!mbar_wait(&bars[st], (uint32_t)(i >> 1) & 1u)) return false;
+    tc_fence_after();
+    const int g = c / G;
+    const uint32_t d = tmem + (uint32_t)(st * kN);
+    const uint64_t ah = umma_desc(smem_u32(a_hi + (size_t)g * kATileBytes));
+    const uint64_t bh = umma_desc(smem_u32(b_hi + st * kBTileBytes));
+    umma_bf16(d, ah, bh, 0u);
+    if (p.split3) {
+      const uint64_t al = umma_desc(smem_u32(a_lo + (size_t)g * kATileBytes));
+      const uint64_t bl = umma_desc(smem_u32(b_lo + st * kBTileBytes));
+      umma_bf16(d, ah, bl, 1u);
+      umma_bf16(d, al, bh, 1u);
+    }
+    umma_commit(&bars[2 + st]);
+    return true;
+  };
   bool ok = true;
+  if (tid == 0 && nc > 0) {
+    issue_copy(0);
+    if (nc > 1) issue_copy(1);
+    ok = issue_mma(0);
+  }
+  ok = __syncthreads_and(ok);
 
-  for (int c = c_begin; c < c_end && ok; c++) {
-    const uint32_t parity = (c - c_begin) & 1;
-    if (tid == 0) {
-      mbar_expect_tx(&bars[0], b_bytes);
-      bulk_copy_g2s(b_hi, p.bpanel_hi + (size_t)c * kBTileBytes, kBTileBytes, &bars[0]);
-      if (p.split3) bulk_copy_g2s(b_lo, p.bpanel_lo + (size_t)c * kBTileBytes, kBTileBytes, &bars[0]);
-    }
-    ok = __syncthreads_and(mbar_wait(&bars[0], parity));
-    if (!ok) break;
-    if (tid == 0) {
-      tc_fence_after();
-      const int g = c / G;
-      const uint64_t ah = umma_desc(smem_u32(a_hi + (size_t)g * kATileBytes));
-      const uint64_t bh = umma_desc(smem_u32(b_hi));
-      umma_bf16(tmem, ah, bh, 0u);
-      if (p.split3) {
-        const uint64_t al = umma_desc(smem_u32(a_lo + (size_t)g * kATileBytes));
-        const uint64_t bl = umma_desc(smem_u32(b_lo));
-        umma_bf16(tmem, ah, bl, 1u);
-        umma_bf16(tmem, al, bh, 1u);
-      }
-      umma_commit(&bars[1]);
-    }
-    ok = __syncthreads_and(mbar_wait(&bars[1], parity));
+  for (int i = 0; i < nc && ok; i++) {
+    const int st = i & 1, c = c_begin + i;
+    bool mine = true;
+    if (tid == 0 && i + 1 < nc) mine = issue_mma(i + 1);  // runs while this chunk drains
+    mine = mine && mbar_wait(&bars[2 + st], (uint32_t)(i >> 1) & 1u);
+    ok = __syncthreads_and(mine);
     if (!ok) break;
     tc_fence_after();
+    if (tid == 0 && i + 2 < nc) issue_copy(i + 2);  // this stage's B tiles are free: MMA i is done
     // Epilogue: row tid of D (TMEM lane tid) -> table[qi][c][0..256)
     const float rq = rn[(size_t)c * kTile + tid];
     const float* pn = p.pnorm + (size_t)c * kN;
     __nv_bfloat16* out = p.tables + ((size_t)qi * p.M + c) * kN;
+    const uint32_t dcol = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(st * kN);
     for (int col = 0; col < kN; col += 16) {
       uint32_t r[16];
-      tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)col, r);
+      tmem_ld16(dcol + (uint32_t)col, r);
       tmem_wait_ld();
       if (qi < p.nq) {
         uint32_t packed[8];
 #pragma unroll
-        for (int i = 0; i < 16; i += 2) {
-          const float v0 = __fmaf_rn(-2.0f, __uint_as_float(r[i]), __fadd_rn(rq, __ldg(pn + col + i)));
-          const float v1 = __fmaf_rn(-2.0f, __uint_as_float(r[i + 1]), __fadd_rn(rq, __ldg(pn + col + i + 1)));
+        for (int j = 0; j < 16; j += 2) {
+          const float v0 = __fmaf_rn(-2.0f, __uint_as_float(r[j]), __fadd_rn(rq, __ldg(pn + col + j)));
+          const float v1 = __fmaf_rn(-2.0f, __uint_as_float(r[j + 1]), __fadd_rn(rq, __ldg(pn + col + j + 1)));
           const __nv_bfloat162 h = __floats2bfloat162_rn(fmaxf(v0, 0.0f), fmaxf(v1, 0.0f));
-          packed[i >> 1] = *reinterpret_cast<const uint32_t*>(&h);
+          packed[j >> 1] = *reinterpret_cast<const uint32_t*>(&h);
         }
         uint4* o = reinterpret_cast<uint4*>(out + col);
         o[0] = make_uint4(packed[0], packed[1], packed[2], packed[3]);
@@ -261,15 +285,15 @@ __global__ void __launch_bounds__(kTile, 1) table_tc_kernel(TcParams p) {
       }
     }
     tc_fence_before();
-    __syncthreads();
+    __syncthreads();  // TMEM columns of stage st are read: chunk i + 2 may overwrite them
   }
   if (!ok && tid == 0) {
     atomicOr(p.err, kErrWaitLimit);
     // let copies and MMAs still in flight land before the memory is released
-    mbar_wait(&bars[0], 0);
-    mbar_wait(&bars[0], 1);
-    mbar_wait(&bars[1], 0);
-    mbar_wait(&bars[1], 1);
+    for (int b = 0; b < 4; b++) {
+      mbar_wait(&bars[b], 0);
+      mbar_wait(&bars[b], 1);
+    }
   }
   tc_fence_before();
   __syncthreads();
@@ -313,7 +337,7 @@ cudaError_t widen_bf16(const __nv_bfloat16* in, float* out, size_t n, cudaStream
 }
 
 size_t table_tc_smem(int M, int groups) {
-  return (size_t)groups * kATileBytes * 2 + (size_t)kBTileBytes * 2 + (size_t)M * kTile * 4 + 16 + 16;
+  return (size_t)groups * kATileBytes * 2 + (size_t)kBTileBytes * 4 + (size_t)M * kTile * 4 + 32 + 16;
 }
 
 // Host-side layout of the B operand tiles (one per chunk) and the centroid norms.
@@ -353,7 +377,7 @@ bool make_tc_panels(const std::vector<float>& pivots, const std::vector<int32_t>
 }
 
 cudaError_t launch_table_tc(const DeviceIndex& ix, int dim, int M, const float* queries, int nq, int split3,
-                            __nv_bfloat16* tables, cudaStream_t stream, const int* nq_dev) {
+                            __nv_bfloat16* tables, cudaStream_t stream, int num_sms, const int* nq_dev) {
   if (!ix.tc_bpanel_hi) return cudaErrorNotSupported;
   TcParams tp{};
   tp.queries = queries;
@@ -376,7 +400,7 @@ cudaError_t launch_table_tc(const DeviceIndex& ix, int dim, int M, const float* 
   cudaError_t e = cudaFuncSetAttribute(table_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   const int tiles = (nq + kTile - 1) / kTile;
-  int split = (2 * 148 + tiles - 1) / tiles;  // enough CTAs to cover the SMs twice
+  int split = (num_sms + tiles - 1) / tiles;  // enough CTAs to cover every SM once
   split = std::max(1, std::min(split, ix.tc_groups));
   table_tc_kernel<<<dim3(tiles, split), kTile, smem, stream>>>(tp);
   return cudaGetLastError();

@@ -250,9 +250,15 @@ int gann_pq_tables(gann_t* h, const float* queries, int nq, int precision, float
  * `streams` batch slots is free (or the oldest has waited max_wait_us) and
  * launches it on that slot's stream, so later arrivals start while earlier
  * batches run and several batches overlap on the device. Each slot's device
- * memory is allocated at start; a submit is refused with GANN_EBUSY while
- * (waiting + running + finished-but-unpolled) requests fill the budget of
- * max_batch * (streams + 1). A result depends only on its query, topk,
+ * memory is allocated at start. Admission is by memory: every request is
+ * charged the device state that its own ef_search and topk need while it is
+ * held (gann_server_request_bytes: its candidate list, its visited cache, its
+ * PQ table, its query and its result row), and a submit is refused with
+ * GANN_EBUSY when the charge of the waiting + running + finished-but-unpolled
+ * requests would pass mem_budget_kib -- so when memory runs short, requests
+ * with a long list are refused while short ones still enter -- or when those
+ * requests already fill the server's max_batch * (streams + 1) request
+ * slots. A result depends only on its query, topk,
  * ef_search and the server options, not on the other requests in its batch.
  * The reference serves one fixed batch per call (src/pure_mem.cu:71-199);
  * no counterpart.
@@ -268,7 +274,8 @@ typedef struct {
   int32_t hash_bits;    /* 0 = sized from ef_max */
   int32_t max_wait_us;  /* a batch smaller than min_batch waits this long for company; 0 = 100 */
   int32_t min_batch;    /* 0 = launch as soon as a slot is free */
-  int32_t reserved[7];
+  int32_t mem_budget_kib; /* admission budget in KiB; 0 = every request slot at (topk_max, ef_max) */
+  int32_t reserved[6];
 } gann_server_opts_t;
 
 typedef struct {
@@ -278,6 +285,9 @@ typedef struct {
 } gann_load_stats_t;
 
 int gann_server_start(gann_t* h, const gann_server_opts_t* opts, gann_server_t** out);
+/* Bytes a request of (topk, ef_search) is charged against the admission
+ * budget of this server. */
+int64_t gann_server_request_bytes(const gann_server_t* s, int topk, int ef_search);
 /* Copy one query (dim floats) in; GANN_EBUSY when the budget is full. */
 int gann_server_submit(gann_server_t* s, const float* query, int topk, int ef_search, uint64_t tag);
 /* Up to max_results finished requests: tags, nns / distances (rows of

@@ -98,3 +98,27 @@ def test_server_open_loop_reports_latency(index):
     assert st["submitted"] > 5000 and st["rejected"] == 0
     assert st["completed"] == st["submitted"]
     assert 0 < st["p50_ms"] <= st["p99_ms"] <= st["p999_ms"] < 1000
+
+
+@pytest.mark.gpu
+def test_admission_by_bytes_refuses_long_lists_before_short_ones(index):
+    """With the byte budget nearly full, a request with a long list (large
+    ef_search, large topk) is refused while a short one still enters; every
+    admitted request is charged gann_server_request_bytes. Nothing is launched
+    during the test (a batch waits for max_batch requests or a minute)."""
+    g, q = index
+    opts = dict(max_batch=64, streams=2, topk_max=100, ef_max=512, precision=gb.PREC_BF16X3,
+                max_wait_us=60_000_000, min_batch=64)
+    srv = gb.Server(g, **opts)
+    big, small = srv.request_bytes(100, 512), srv.request_bytes(1, 32)
+    srv.stop()
+    assert big - small > 2048 and small > 0
+    cap = (2 * big + small + (big - small) // 2) // 1024 * 1024  # two long requests, then room for short ones only
+    srv = gb.Server(g, mem_budget_kib=cap // 1024, **opts)
+    assert [srv.submit(q[i], 100, 512, i) for i in range(4)] == [True, True, False, False]
+    n_small = (cap - 2 * big) // small
+    assert n_small >= 1
+    took = [srv.submit(q[10 + i], 1, 32, 10 + i) for i in range(n_small + 2)]
+    assert took == [True] * n_small + [False, False]
+    assert not srv.submit(q[50], 100, 512, 50)
+    srv.stop()
