@@ -194,6 +194,7 @@ __global__ void __launch_bounds__(256) prune_kernel(PruneArgs a) {
 
 template <class T, int KP>
 cudaError_t launch_prune(PruneArgs a, cudaStream_t s) {
+  if (!a.x || !a.cand || !a.out) return cudaErrorInvalidValue;
   const size_t per_warp = (size_t)a.warp_words * 4;
   int wpb = (int)((160 * 1024) / per_warp);
   wpb = wpb < 1 ? 1 : (wpb > 8 ? 8 : wpb);
@@ -248,6 +249,7 @@ extern "C" int gann_build_prune(const void* d_x, int dtype, int64_t n, int dim, 
   a.R = R;
   a.alpha = alpha;
   a.warp_words = (K + 1) * a.stride + 3 * kPruneMaxK;
+  a.out = d_out;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const cudaError_t e = dtype == GANN_UINT8 ? launch_prune_t<uint8_t>(a, s) : launch_prune_t<float>(a, s);
   if (e != cudaSuccess)
