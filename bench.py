@@ -569,6 +569,58 @@ def measure_mix(g, q, gt, args, world, flush, local, W):
     return out
 
 
+def precision_study(g, meta, runners, res, q_dev, gt, k, n_sample=1000):
+    """Table and rerank error of every precision against FP64 on a sample of
+    the queries, and every form's recall at the plain form's L (the L where the
+    reference semantics reach the target)."""
+    import torch
+
+    import gustann_b200 as gb
+    from gustann_b200.indexing import formats
+
+    q = meta["queries"][:n_sample].astype(np.float32)
+    piv, mu, co = formats.read_pq_pivots(meta["pq_prefix"])
+    r = q.astype(np.float64) - mu.astype(np.float64)
+    P = piv.astype(np.float64)
+    M = len(co) - 1
+    t64 = np.zeros((q.shape[0], M, 256))
+    for c in range(M):
+        b, e = int(co[c]), int(co[c + 1])
+        t64[:, c, :] = ((r[:, None, b:e] - P[None, :, b:e]) ** 2).sum(-1)
+    scale = np.maximum(t64.max(axis=2, keepdims=True), 1e-30)  # per (query, chunk) range
+    table = {}
+    for name, prec in (("fp32", gb.PREC_FP32), ("bf16_cc", gb.PREC_BF16_CC), ("bf16x3", gb.PREC_BF16X3),
+                       ("bf16", gb.PREC_BF16)):
+        rel = np.abs(g.pq_tables(q, prec).astype(np.float64) - t64) / scale
+        table[name] = {"max": float(rel.max()), "mean": float(rel.mean()), "p99": float(np.quantile(rel, 0.99))}
+    out = {"queries": int(q.shape[0]),
+           "table_error_vs_fp64": table,
+           "table_error_unit": "|table - FP64 table| / (the FP64 table's largest entry of that query and chunk)"}
+    L_plain = res["plain"]["L"] if "plain" in res else None
+    rerank, recall_at = {}, {}
+    dtype = np.uint8 if meta["kind"] == "u8" else np.float32
+    for f in [f for f in ("plain", "batched_bf16", "batched_bf16x3", "batched_fp32") if f in runners]:
+        run = runners[f]
+        run.run(L_plain or res[f]["L"])
+        torch.cuda.synchronize()
+        g.check()
+        ids, dis, fnd = run.ids.cpu().numpy(), run.dis.cpu().numpy(), run.fnd.cpu().numpy()
+        recall_at[f] = calc_recall(ids, gt, k)
+        sel = np.arange(min(200, n_sample))
+        vi = ids[sel].reshape(-1)
+        vec = formats.read_index_vectors(meta["index_file"], dtype, vi).astype(np.float64).reshape(len(sel), k, -1)
+        d64 = ((vec - meta["queries"][sel].astype(np.float64)[:, None, :]) ** 2).sum(-1)
+        ok = np.arange(k)[None, :] < fnd[sel][:, None]
+        rel = np.abs(dis[sel].astype(np.float64) - d64) / np.maximum(d64, 1e-30)
+        rerank[f] = float(rel[ok].max()) if ok.any() else None
+    out["rerank_error_vs_fp64"] = {"max_relative": rerank, "queries": int(min(200, n_sample)),
+                                   "ids": "the k returned ids of each query"}
+    if L_plain:
+        out["recall_at_plain_L"] = {"L": L_plain, **recall_at}
+        out["recall_gap_to_plain"] = {f: recall_at[f] - recall_at["plain"] for f in recall_at if f != "plain"}
+    return out
+
+
 def plain_parity(g, meta, q_dev, k):
     """The plain form against the reference kernel's own outputs on the same
     index and queries (saved by the reference arm), id for id."""
@@ -699,6 +751,8 @@ def _run_ours(args, rank, world, local):
     }
     if "plain" in res and head != "plain":
         out["speedup_vs_plain"] = r["qps"] / res["plain"]["qps"]
+    if args.precision:
+        out["precision"] = precision_study(g, meta, runners, res, q, gt, k)
     par = plain_parity(g, meta, q, k)
     if par is not None:
         out["parity"] = par
@@ -829,6 +883,8 @@ def main():
     ap.add_argument("--beam", type=int, default=0, help="0 = autotune (gann_autotune)")
     ap.add_argument("--tune-L", type=int, default=384)
     ap.add_argument("--batch", type=int, default=0, help="queries per step (default: all --nq)")
+    ap.add_argument("--no-precision", dest="precision", action="store_false",
+                    help="skip the table / rerank error study against FP64")
     ap.add_argument("--no-mix", dest="mix", action="store_false",
                     help="skip the mixed-L/k step of the batching config")
     ap.add_argument("--serve-rates", default="100000,500000,1000000,1500000,2000000",

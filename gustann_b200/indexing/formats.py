@@ -209,6 +209,36 @@ def read_disk_index(path: str, dtype) -> DiskIndex:
                      adj[:, 1:].astype(np.int32))
 
 
+def read_index_vectors(path: str, dtype, ids: np.ndarray) -> np.ndarray:
+    """The vectors of the given node ids from a _disk.index, read through a
+    memory map page by page (no full load)."""
+    dtype = np.dtype(dtype)
+    head = np.fromfile(path, dtype=np.uint8, count=8 + 5 * 8)
+    n, dim, medoid, nl, npp = struct.unpack_from("<5Q", head.tobytes(), 8)
+    mm = np.memmap(path, dtype=np.uint8, mode="r")
+    ids = np.asarray(ids, dtype=np.int64).reshape(-1)
+    off = PAGE + (ids // npp) * PAGE + (ids % npp) * nl
+    nbytes = dim * dtype.itemsize
+    rows = np.stack([np.asarray(mm[o:o + nbytes]) for o in off]) if len(ids) else np.zeros((0, nbytes), np.uint8)
+    return np.ascontiguousarray(rows).view(dtype).reshape(len(ids), dim)
+
+
+def read_pq_pivots(prefix: str):
+    """(pivots 256 x dim float32, centroid dim float32, chunk offsets M + 1
+    uint32) from <prefix>_pivots.bin, either offsets-table size (4 or the
+    legacy 5, PQSearch::read_data, src/pq_search.cu:74-100)."""
+    raw = open(prefix + "_pivots.bin", "rb").read()
+    nr = struct.unpack_from("<i", raw, 0)[0]
+    offs = np.frombuffer(raw, np.uint64, count=nr, offset=8)
+    rows, dim = struct.unpack_from("<ii", raw, int(offs[0]))
+    piv = np.frombuffer(raw, np.float32, count=256 * dim, offset=int(offs[0]) + 8).reshape(256, dim)
+    mu = np.frombuffer(raw, np.float32, count=dim, offset=int(offs[1]) + 8)
+    co_off = int(offs[3 if nr == 5 else 2])
+    m1 = struct.unpack_from("<i", raw, co_off)[0]
+    co = np.frombuffer(raw, np.uint32, count=m1, offset=co_off + 8)
+    return piv.copy(), mu.copy(), co.copy()
+
+
 def write_vecs(path: str, arr: np.ndarray) -> None:
     """fvecs (float32), ivecs (int32) or bvecs (uint8): per row a 4-byte dim then the row."""
     arr = np.ascontiguousarray(arr)

@@ -153,3 +153,19 @@ def test_prune_kernel_follows_the_rule(kind):
     else:
         same = (got == want).all(1).float().mean().item()
         assert same > 0.98, same
+
+
+@pytest.mark.parametrize("name", ["u8_nav", "f32_nav"])
+def test_page_readers_match_the_full_parse(tmp_path, name):
+    """read_index_vectors (memory-mapped, per node) and read_pq_pivots give the
+    same values as the full-file parse and the writer's inputs."""
+    from make_fixtures import unpack
+
+    m = unpack(name, tmp_path)
+    dt = np.uint8 if m["dtype"] == 0 else np.float32
+    di = formats.read_disk_index(m["index_file"], dt)
+    ids = np.array([0, 5, di.n - 1, 17, 5])
+    np.testing.assert_array_equal(formats.read_index_vectors(m["index_file"], dt, ids), di.data[ids])
+    piv, mu, co = formats.read_pq_pivots(m["pq_prefix"])
+    assert piv.shape == (256, di.dim) and mu.shape == (di.dim,)
+    assert co[0] == 0 and co[-1] == di.dim and np.all(np.diff(co.astype(np.int64)) >= 1)
