@@ -119,6 +119,27 @@ def kmeans(x: torch.Tensor, k: int, iters: int, seed: int, sample: int) -> torch
     return cent
 
 
+def leaf_batches(q_counts: np.ndarray, pool_sizes: np.ndarray, budget: int) -> list[tuple[int, int]]:
+    """Groups of consecutive leaves (given in order of falling pool size) for
+    one batched GEMM each: (first, count). The first leaf of a group sets the
+    pool width, and leaves are added while the distance block count x
+    (largest query count so far) x (pool width) stays within the budget; a
+    single leaf always forms a group."""
+    out = []
+    i, n = 0, len(q_counts)
+    while i < n:
+        sp = max(1, int(pool_sizes[i]))
+        G, sq = 0, 0
+        while i + G < n:
+            mq = max(sq, int(q_counts[i + G]))
+            if G and (G + 1) * mq * sp > budget:
+                break
+            sq, G = mq, G + 1
+        out.append((i, G))
+        i += G
+    return out
+
+
 def leaf_candidates(x: torch.Tensor, K: int, leaf: int, seed: int, log=None,
                     budget: int = 1 << 29) -> torch.Tensor:
     """K nearest neighbours of every point inside its leaf's pool (n x K int32,
@@ -146,14 +167,9 @@ def leaf_candidates(x: torch.Tensor, K: int, leaf: int, seed: int, log=None,
     order = torch.argsort(pool, descending=True)
     order = order[c1[order] > 0]
     c1h, poolh, orderh = c1.cpu().numpy(), pool.cpu().numpy(), order.cpu().numpy()
-    i = 0
     inf = float("inf")
-    while i < len(orderh):
-        sq, sp = int(c1h[orderh[i]]), int(poolh[orderh[i]])
-        per = max(1, sq) * max(1, sp)
-        G = max(1, min(len(orderh) - i, budget // per))
+    for i, G in leaf_batches(c1h[orderh], poolh[orderh], budget):
         Lb = order[i:i + G]
-        i += G
         q_cnt, p_cnt, c1b = c1[Lb], pool[Lb], c1[Lb]
         Sq, Sp = int(q_cnt.max()), int(p_cnt.max())
         ar_q = torch.arange(Sq, device=dev)

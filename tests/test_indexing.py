@@ -169,3 +169,23 @@ def test_page_readers_match_the_full_parse(tmp_path, name):
     piv, mu, co = formats.read_pq_pivots(m["pq_prefix"])
     assert piv.shape == (256, di.dim) and mu.shape == (di.dim,)
     assert co[0] == 0 and co[-1] == di.dim and np.all(np.diff(co.astype(np.int64)) >= 1)
+
+
+def test_leaf_batches_respect_the_distance_budget():
+    """Every group's block (leaves x largest query count x pool width) stays
+    within the budget unless the group is a single leaf, and the groups cover
+    every leaf once, in order -- including a small first leaf followed by
+    leaves with many more queries."""
+    from gustann_b200.indexing import ivf
+
+    rng = np.random.default_rng(3)
+    pool = np.sort(rng.integers(1, 30000, size=500))[::-1]
+    q = np.minimum(pool, rng.integers(0, 30000, size=500))
+    q[0] = 1  # a pool made almost only of second-nearest members
+    budget = 1 << 26
+    groups = ivf.leaf_batches(q, pool, budget)
+    assert [i for i, _ in groups] == list(np.cumsum([0] + [g for _, g in groups[:-1]]))
+    assert sum(g for _, g in groups) == 500
+    for i, g in groups:
+        block = g * max(1, int(q[i:i + g].max())) * max(1, int(pool[i]))
+        assert g == 1 or block <= budget

@@ -75,7 +75,7 @@ def test_noalloc_defaults_follow_the_autotuned_handle(golden):
     g = _open(meta)
     dq = torch.from_numpy(meta["queries"]).cuda()
     g.autotune(dq.data_ptr(), dq.shape[0], 10, 48, gb.PREC_BF16)
-    _two_calls(g, meta, gb.PREC_BF16, None, 0, 0)
+    _two_calls(g, meta, gb.PREC_BF16X3, None, 0, 0)  # opts NULL: split-BF16 tensor-core tables
     _two_calls(g, meta, gb.PREC_BF16, gb.GustANN._opts(gb.PREC_BF16, 0, 0), 0, 0)
     g.close()
 
