@@ -234,6 +234,111 @@ def add_reverse(x: torch.Tensor, g: torch.Tensor, R: int, alpha: float, in_cap: 
     return out
 
 
+def far_edges(x: torch.Tensor, per_part: int = 2, parts: int = 8, part_size: int = 256, seed: int = 5,
+              log=None) -> torch.Tensor:
+    """Long edges for a pivot graph: the rows are k-means partitioned (about
+    part_size points per centre) and every point gets its per_part nearest
+    points in each of the `parts` partitions whose centres lie nearest to its
+    own partition's centre (its own excluded). Returns n x (parts * per_part)
+    int64 ids, -1 padded. On data made of well-separated clusters, k-means with
+    fewer centres than clusters keeps clusters whole, so these edges cross to
+    the neighbouring clusters in several directions -- the edges a greedy walk
+    needs to move between clusters, which nearest-first pruning never keeps
+    once a cluster holds more than R points."""
+    n = x.shape[0]
+    dev = x.device
+    k = max(2, n // part_size)
+    parts = min(parts, k - 1)
+    t0 = time.time()
+    with _tf32():
+        cent = kmeans(x, k, iters=8, seed=seed, sample=min(n, 64 * k))
+        a1, _ = assign2(x, cent)
+    o1 = torch.argsort(a1)
+    c1 = torch.bincount(a1, minlength=k)
+    s1 = torch.cumsum(c1, 0) - c1
+    cc = builder.sqdist(cent, cent)
+    cc.fill_diagonal_(float("inf"))
+    near = torch.topk(cc, parts, dim=1, largest=False).indices  # k x parts
+    out = torch.full((n, parts * per_part), -1, dtype=torch.long, device=dev)
+    c1h, s1h, nearh = c1.cpu().numpy(), s1.cpu().numpy(), near.cpu().numpy()
+    smax = int(c1h.max())
+    ar = torch.arange(smax, device=dev)
+    for c in range(k):
+        if c1h[c] == 0:
+            continue
+        q = o1[s1h[c]: s1h[c] + c1h[c]]
+        segs = nearh[c]
+        cnt = torch.from_numpy(c1h[segs]).to(dev)
+        pos = torch.from_numpy(s1h[segs]).to(dev)[:, None] + ar[None, :]
+        pool = o1[pos.clamp(max=n - 1)]                       # parts x smax
+        valid = ar[None, :] < cnt[:, None]
+        D = builder.sqdist(x[q], x[pool.reshape(-1)]).view(q.numel(), parts, smax)
+        D.masked_fill_(~valid[None], float("inf"))
+        kk = min(per_part, smax)
+        v, j = torch.topk(D, kk, dim=2, largest=False)         # |q| x parts x kk
+        ids = torch.gather(pool[None].expand(q.numel(), parts, smax), 2, j)
+        ids = torch.where(torch.isinf(v), torch.full_like(ids, -1), ids)
+        out[q, : parts * kk] = ids.reshape(q.numel(), -1)
+    if log:
+        log(f"far edges: {k} partitions, {parts} x {per_part} per point, {time.time() - t0:.1f} s")
+    return out
+
+
+def pivot_graph(x: torch.Tensor, near: torch.Tensor, R: int, seed: int = 5, log=None) -> torch.Tensor:
+    """Rows of a pivot graph that mixes near and far edges: the first R/2
+    near neighbours (a Vamana graph's rows, nearest first) interleaved with
+    R/2 far edges (far_edges), repeats dropped, near edges filling any slot
+    left. Interleaving keeps both kinds inside the first slots that the entry
+    walk reads (28 of at most 32, src/impl/nav.cuh:11-12)."""
+    n = x.shape[0]
+    half = R // 2
+    far = far_edges(x, per_part=2, parts=max(1, half // 2), seed=seed, log=log)[:, :half]
+    near = near.long()
+    inter = torch.stack([near[:, :half], torch.cat([far, torch.full((n, half - far.shape[1]), -1, device=x.device,
+                                                                     dtype=torch.long)], 1)], 2).reshape(n, 2 * half)
+    cand = torch.cat([inter, near[:, half:]], 1)
+    # drop repeats (keep the first copy) and self edges, then compact
+    self_ = cand == torch.arange(n, device=x.device)[:, None]
+    o = torch.argsort(cand, dim=1, stable=True)
+    sc = torch.gather(cand, 1, o)
+    dup = torch.zeros_like(sc, dtype=torch.bool)
+    dup[:, 1:] = sc[:, 1:] == sc[:, :-1]
+    rep = torch.zeros_like(dup).scatter_(1, o, dup)
+    cand = torch.where(rep | self_, torch.full_like(cand, -1), cand)
+    cand = torch.gather(cand, 1, torch.argsort((cand < 0).to(torch.int8), dim=1, stable=True))
+    return cand[:, :R]
+
+
+def repair_orphans(g: torch.Tensor, passes: int = 3, log=None) -> torch.Tensor:
+    """Give every node an in-edge: a node that no row lists is written into
+    the row of its own nearest neighbour (the first entry of its row), in the
+    last slots, displacing that row's farthest neighbours; rows are compacted
+    again. A displaced node left without in-edges is repaired in the next pass."""
+    n, R = g.shape
+    dev = g.device
+    for _ in range(passes):
+        indeg = torch.bincount(g[g >= 0].long(), minlength=n)
+        orph = torch.nonzero(indeg == 0).squeeze(1)
+        orph = orph[g[orph, 0] >= 0]
+        if orph.numel() == 0:
+            break
+        tgt = g[orph, 0].long()
+        o = torch.argsort(tgt, stable=True)
+        tgt, orph = tgt[o], orph[o]
+        uniq, cnt = torch.unique_consecutive(tgt, return_counts=True)
+        start = torch.cumsum(cnt, 0) - cnt
+        rank = torch.arange(tgt.numel(), device=dev) - torch.repeat_interleave(start, cnt)
+        keep = rank < R // 4
+        tgt, orph, rank = tgt[keep], orph[keep], rank[keep]
+        g[tgt, R - 1 - rank] = orph.to(g.dtype)
+        rows = torch.unique(tgt)
+        sub = g[rows]
+        g[rows] = torch.gather(sub, 1, torch.argsort((sub < 0).to(torch.int8), dim=1, stable=True))
+        if log:
+            log(f"orphan repair: {int(indeg.eq(0).sum())} nodes without in-edges, {tgt.numel()} linked")
+    return g
+
+
 def embed_pivots(g: torch.Tensor, piv: torch.Tensor, nav_graph: torch.Tensor, nav_slots: int) -> torch.Tensor:
     """Put up to nav_slots pivot-graph neighbours (mapped to global ids) at the
     end of every sampled point's row, after its nearest R - nav_slots
@@ -260,7 +365,7 @@ def embed_pivots(g: torch.Tensor, piv: torch.Tensor, nav_graph: torch.Tensor, na
 
 
 def build(x: torch.Tensor, R: int, alpha: float = 1.2, K: int | None = None, leaf: int = 4096, seed: int = 7,
-          pivots: np.ndarray | None = None, nav_graph: np.ndarray | None = None, nav_slots: int = 8,
+          pivots: np.ndarray | None = None, nav_graph: np.ndarray | None = None, nav_slots: int = 16,
           log=None) -> tuple[torch.Tensor, torch.Tensor, int, dict]:
     """Graph over the rows of x (uint8 or float32, on the GPU for large n).
     Returns (adjacency n x R int32 on x's device, -1 padded; degrees; medoid;
@@ -287,6 +392,7 @@ def build(x: torch.Tensor, R: int, alpha: float = 1.2, K: int | None = None, lea
         piv = torch.from_numpy(np.asarray(pivots, dtype=np.int64)).to(x.device)
         ng = torch.from_numpy(np.asarray(nav_graph, dtype=np.int64)).to(x.device)
         g = embed_pivots(g, piv, ng, min(nav_slots, R // 2))
+    g = repair_orphans(g, log=log)
     deg = (g >= 0).sum(1).to(torch.int32)
     indeg = torch.bincount(g[g >= 0].long(), minlength=x.shape[0])
     timings["no_in_edges"] = int((indeg == 0).sum())

@@ -189,3 +189,32 @@ def test_leaf_batches_respect_the_distance_budget():
     for i, g in groups:
         block = g * max(1, int(q[i:i + g].max())) * max(1, int(pool[i]))
         assert g == 1 or block <= budget
+
+
+def test_far_edges_cross_clusters_and_orphans_are_repaired():
+    """On a mixture with more points per cluster than pivot-graph slots, the
+    far edges of every point lead into other clusters (several of them), and
+    repair_orphans leaves no node without an in-edge."""
+    from gustann_b200.indexing import ivf
+
+    base, _ = synth.make("u8", 4000, 64, 40, 1, backend="numpy")  # 100 points per cluster
+    x = torch.from_numpy(base)
+    C = torch.from_numpy(synth.centres("u8", 64, 40))
+    lab = builder.sqdist(x, C).argmin(1)
+    far = ivf.far_edges(x, per_part=2, parts=4, part_size=256)
+    ok = far >= 0
+    assert ok.float().mean() > 0.95
+    other = (lab[far.clamp_min(0)] != lab[:, None]) & ok
+    assert other.sum(1).float().mean() > 6.0  # of 8 far edges
+    dirs = [len(set(lab[far[i][ok[i]]].tolist())) for i in range(0, 4000, 37)]
+    assert np.mean(dirs) >= 3
+    g = torch.full((50, 4), -1, dtype=torch.long)
+    for i in range(50):
+        g[i, 0] = (i + 1) % 50
+        if i % 2 == 0:
+            g[i, 1] = (i + 2) % 50
+    g[:, 0] = torch.where(torch.arange(50) % 5 == 0, torch.full((50,), 1), g[:, 0])
+    g = ivf.repair_orphans(g)
+    indeg = torch.bincount(g[g >= 0], minlength=50)
+    assert (indeg > 0).all()
+    assert ((g >= 0).int().diff(dim=1) <= 0).all()  # rows stay compact
