@@ -49,7 +49,7 @@ WORKLOADS = {
     # the C2 generator and graph shape at a tenth of the size (10,000 points per cluster as in c2)
     "c2_10m": ("u8", 10_000_000, 128, 1_000, 32, 32, 100_000),
 }
-L_LADDER = [16, 24, 32, 48, 64, 96, 128, 160, 192, 256, 320, 384, 448, 512, 640, 768, 1024, 1536, 2048]
+L_LADDER = [16, 24, 32, 48, 64, 96, 128, 160, 192, 256, 320, 384, 448, 512, 640, 768, 1024, 1536, 2048, 3072, 4096]
 MIX_L, MIX_K = (32, 64, 128, 256), (1, 10, 100)
 
 
@@ -887,7 +887,7 @@ def main():
                     help="skip the table / rerank error study against FP64")
     ap.add_argument("--no-mix", dest="mix", action="store_false",
                     help="skip the mixed-L/k step of the batching config")
-    ap.add_argument("--serve-rates", default="100000,500000,1000000,1500000,2000000",
+    ap.add_argument("--serve-rates", default="250000,500000,1000000,2000000,4000000",
                     help="offered QPS of the open-loop serving sweep ('' = skip)")
     ap.add_argument("--serve-seconds", type=float, default=1.0)
     ap.add_argument("--serve-batch", type=int, default=1024)

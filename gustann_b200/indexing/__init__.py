@@ -69,13 +69,6 @@ def build_index(base, out_dir: str, R: int, M: int = 32, alpha: float = 1.2, nav
         ids = sample_pivots(n, min(nav_samples, n))
         sub = x[torch.from_numpy(ids.astype(np.int64)).to(x.device)]
         ng, ndeg, nmed = builder.build(sub, nav_R, alpha, seed=seed + 1)
-        if large:  # near + far edges, so that walks can move between clusters
-            from . import ivf
-
-            ng_t = ivf.pivot_graph(sub, torch.from_numpy(ng.astype(np.int64)).to(x.device), nav_R, seed=seed + 2,
-                                   log=log)
-            ndeg = (ng_t >= 0).sum(1).to(torch.int32).cpu().numpy()
-            ng = ng_t.to(torch.int32).cpu().numpy()
         if int(ndeg.min()) < 3:
             raise RuntimeError("pivot graph has a node with fewer than 3 neighbours")
         nav = (ids, sub, ng, ndeg, nmed)

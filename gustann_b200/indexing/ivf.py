@@ -168,14 +168,26 @@ def leaf_candidates(x: torch.Tensor, K: int, leaf: int, seed: int, log=None,
     order = order[c1[order] > 0]
     c1h, poolh, orderh = c1.cpu().numpy(), pool.cpu().numpy(), order.cpu().numpy()
     inf = float("inf")
+    groups = []
     for i, G in leaf_batches(c1h[orderh], poolh[orderh], budget):
+        sp = max(1, int(poolh[orderh[i]]))
+        if G == 1 and int(c1h[orderh[i]]) * sp > budget:  # one leaf too large for one block: split its queries
+            step = max(1, budget // sp)
+            groups += [(i, 1, a, min(int(c1h[orderh[i]]), a + step)) for a in range(0, int(c1h[orderh[i]]), step)]
+        else:
+            groups.append((i, G, 0, None))
+    for i, G, qa, qb in groups:
         Lb = order[i:i + G]
         q_cnt, p_cnt, c1b = c1[Lb], pool[Lb], c1[Lb]
+        q_off = torch.zeros_like(q_cnt)
+        if qb is not None:  # a slice [qa, qb) of one large leaf's queries
+            q_off = torch.full_like(q_cnt, qa)
+            q_cnt = torch.full_like(q_cnt, qb - qa)
         Sq, Sp = int(q_cnt.max()), int(p_cnt.max())
         ar_q = torch.arange(Sq, device=dev)
         ar_p = torch.arange(Sp, device=dev)
         qmask = ar_q[None, :] < q_cnt[:, None]
-        qi = o1[(s1[Lb][:, None] + ar_q[None, :]).clamp(max=n - 1)]
+        qi = o1[(s1[Lb][:, None] + q_off[:, None] + ar_q[None, :]).clamp(max=n - 1)]
         from1 = ar_p[None, :] < c1b[:, None]
         idx1 = (s1[Lb][:, None] + ar_p[None, :]).clamp(max=n - 1)
         idx2 = (s2[Lb][:, None] + ar_p[None, :] - c1b[:, None]).clamp(0, n - 1)
@@ -234,81 +246,6 @@ def add_reverse(x: torch.Tensor, g: torch.Tensor, R: int, alpha: float, in_cap: 
     return out
 
 
-def far_edges(x: torch.Tensor, per_part: int = 2, parts: int = 8, part_size: int = 256, seed: int = 5,
-              log=None) -> torch.Tensor:
-    """Long edges for a pivot graph: the rows are k-means partitioned (about
-    part_size points per centre) and every point gets its per_part nearest
-    points in each of the `parts` partitions whose centres lie nearest to its
-    own partition's centre (its own excluded). Returns n x (parts * per_part)
-    int64 ids, -1 padded. On data made of well-separated clusters, k-means with
-    fewer centres than clusters keeps clusters whole, so these edges cross to
-    the neighbouring clusters in several directions -- the edges a greedy walk
-    needs to move between clusters, which nearest-first pruning never keeps
-    once a cluster holds more than R points."""
-    n = x.shape[0]
-    dev = x.device
-    k = max(2, n // part_size)
-    parts = min(parts, k - 1)
-    t0 = time.time()
-    with _tf32():
-        cent = kmeans(x, k, iters=8, seed=seed, sample=min(n, 64 * k))
-        a1, _ = assign2(x, cent)
-    o1 = torch.argsort(a1)
-    c1 = torch.bincount(a1, minlength=k)
-    s1 = torch.cumsum(c1, 0) - c1
-    cc = builder.sqdist(cent, cent)
-    cc.fill_diagonal_(float("inf"))
-    near = torch.topk(cc, parts, dim=1, largest=False).indices  # k x parts
-    out = torch.full((n, parts * per_part), -1, dtype=torch.long, device=dev)
-    c1h, s1h, nearh = c1.cpu().numpy(), s1.cpu().numpy(), near.cpu().numpy()
-    smax = int(c1h.max())
-    ar = torch.arange(smax, device=dev)
-    for c in range(k):
-        if c1h[c] == 0:
-            continue
-        q = o1[s1h[c]: s1h[c] + c1h[c]]
-        segs = nearh[c]
-        cnt = torch.from_numpy(c1h[segs]).to(dev)
-        pos = torch.from_numpy(s1h[segs]).to(dev)[:, None] + ar[None, :]
-        pool = o1[pos.clamp(max=n - 1)]                       # parts x smax
-        valid = ar[None, :] < cnt[:, None]
-        D = builder.sqdist(x[q], x[pool.reshape(-1)]).view(q.numel(), parts, smax)
-        D.masked_fill_(~valid[None], float("inf"))
-        kk = min(per_part, smax)
-        v, j = torch.topk(D, kk, dim=2, largest=False)         # |q| x parts x kk
-        ids = torch.gather(pool[None].expand(q.numel(), parts, smax), 2, j)
-        ids = torch.where(torch.isinf(v), torch.full_like(ids, -1), ids)
-        out[q, : parts * kk] = ids.reshape(q.numel(), -1)
-    if log:
-        log(f"far edges: {k} partitions, {parts} x {per_part} per point, {time.time() - t0:.1f} s")
-    return out
-
-
-def pivot_graph(x: torch.Tensor, near: torch.Tensor, R: int, seed: int = 5, log=None) -> torch.Tensor:
-    """Rows of a pivot graph that mixes near and far edges: the first R/2
-    near neighbours (a Vamana graph's rows, nearest first) interleaved with
-    R/2 far edges (far_edges), repeats dropped, near edges filling any slot
-    left. Interleaving keeps both kinds inside the first slots that the entry
-    walk reads (28 of at most 32, src/impl/nav.cuh:11-12)."""
-    n = x.shape[0]
-    half = R // 2
-    far = far_edges(x, per_part=2, parts=max(1, half // 2), seed=seed, log=log)[:, :half]
-    near = near.long()
-    inter = torch.stack([near[:, :half], torch.cat([far, torch.full((n, half - far.shape[1]), -1, device=x.device,
-                                                                     dtype=torch.long)], 1)], 2).reshape(n, 2 * half)
-    cand = torch.cat([inter, near[:, half:]], 1)
-    # drop repeats (keep the first copy) and self edges, then compact
-    self_ = cand == torch.arange(n, device=x.device)[:, None]
-    o = torch.argsort(cand, dim=1, stable=True)
-    sc = torch.gather(cand, 1, o)
-    dup = torch.zeros_like(sc, dtype=torch.bool)
-    dup[:, 1:] = sc[:, 1:] == sc[:, :-1]
-    rep = torch.zeros_like(dup).scatter_(1, o, dup)
-    cand = torch.where(rep | self_, torch.full_like(cand, -1), cand)
-    cand = torch.gather(cand, 1, torch.argsort((cand < 0).to(torch.int8), dim=1, stable=True))
-    return cand[:, :R]
-
-
 def repair_orphans(g: torch.Tensor, passes: int = 3, log=None) -> torch.Tensor:
     """Give every node an in-edge: a node that no row lists is written into
     the row of its own nearest neighbour (the first entry of its row), in the
@@ -342,13 +279,19 @@ def repair_orphans(g: torch.Tensor, passes: int = 3, log=None) -> torch.Tensor:
 def embed_pivots(g: torch.Tensor, piv: torch.Tensor, nav_graph: torch.Tensor, nav_slots: int) -> torch.Tensor:
     """Put up to nav_slots pivot-graph neighbours (mapped to global ids) at the
     end of every sampled point's row, after its nearest R - nav_slots
-    neighbours; ids already in the row are not repeated."""
+    neighbours; ids already in the row are not repeated. The pivot graph's
+    rows are in distance order, so they are read from the far end: the long
+    edges that the pivot graph's searches created, which cross between
+    clusters, are the ones a walk in the main graph lacks."""
     if nav_slots <= 0 or piv.numel() == 0:
         return g
     R = g.shape[1]
     keep = R - nav_slots
     rows = g[piv].long()  # P x R, kept neighbours first
     ng = nav_graph.long()
+    ndeg = (ng >= 0).sum(1)
+    back = ndeg[:, None] - 1 - torch.arange(ng.shape[1], device=ng.device)[None, :]
+    ng = torch.where(back >= 0, torch.gather(ng, 1, back.clamp_min(0)), torch.full_like(ng, -1))  # farthest first
     glob = torch.where(ng >= 0, piv[ng.clamp_min(0)], torch.full_like(ng, -1))
     dup = (glob[:, :, None] == rows[:, None, :keep]).any(-1) | (glob < 0) | (glob == piv[:, None])
     # first nav_slots non-duplicate entries, in pivot-graph order

@@ -191,30 +191,29 @@ def test_leaf_batches_respect_the_distance_budget():
         assert g == 1 or block <= budget
 
 
-def test_far_edges_cross_clusters_and_orphans_are_repaired():
-    """On a mixture with more points per cluster than pivot-graph slots, the
-    far edges of every point lead into other clusters (several of them), and
-    repair_orphans leaves no node without an in-edge."""
+def test_orphans_are_repaired():
+    """repair_orphans leaves no node without an in-edge and rows compact."""
     from gustann_b200.indexing import ivf
 
-    base, _ = synth.make("u8", 4000, 64, 40, 1, backend="numpy")  # 100 points per cluster
-    x = torch.from_numpy(base)
-    C = torch.from_numpy(synth.centres("u8", 64, 40))
-    lab = builder.sqdist(x, C).argmin(1)
-    far = ivf.far_edges(x, per_part=2, parts=4, part_size=256)
-    ok = far >= 0
-    assert ok.float().mean() > 0.95
-    other = (lab[far.clamp_min(0)] != lab[:, None]) & ok
-    assert other.sum(1).float().mean() > 6.0  # of 8 far edges
-    dirs = [len(set(lab[far[i][ok[i]]].tolist())) for i in range(0, 4000, 37)]
-    assert np.mean(dirs) >= 3
     g = torch.full((50, 4), -1, dtype=torch.long)
     for i in range(50):
         g[i, 0] = (i + 1) % 50
         if i % 2 == 0:
             g[i, 1] = (i + 2) % 50
     g[:, 0] = torch.where(torch.arange(50) % 5 == 0, torch.full((50,), 1), g[:, 0])
+    assert (torch.bincount(g[g >= 0], minlength=50) == 0).any()
     g = ivf.repair_orphans(g)
     indeg = torch.bincount(g[g >= 0], minlength=50)
     assert (indeg > 0).all()
     assert ((g >= 0).int().diff(dim=1) <= 0).all()  # rows stay compact
+
+
+def test_embedded_pivot_edges_are_the_far_end_of_the_pivot_rows():
+    from gustann_b200.indexing import ivf
+
+    g = torch.arange(40).reshape(10, 4).long() + 100  # 10 nodes, R 4, neighbours 100+
+    piv = torch.tensor([2, 5])
+    nav = torch.tensor([[1, 0, -1], [0, -1, -1]])  # pivot-graph rows (local ids), nearest first
+    out = ivf.embed_pivots(g.clone(), piv, nav, 2)
+    assert out[2].tolist() == [108, 109, 5, -1]  # kept 2 nearest, then pivot 1 (= node 5); its own id is dropped
+    assert out[5].tolist() == [120, 121, 2, -1]
