@@ -43,7 +43,7 @@ def _np(x):
 def build_index(base, out_dir: str, R: int, M: int = 32, alpha: float = 1.2, nav_samples: int | None = None,
                 nav_R: int = 32, device=None, n_coarse: int | None = None, nprobe: int = 4,
                 pq_train: int = 1 << 18, seed: int = 7, legacy_pq: bool = False, method: str = "auto",
-                leaf: int = 4096, log=None) -> IndexFiles:
+                leaf: int = 4096, nav_L_build: int = 100, log=None) -> IndexFiles:
     """Build and write every file of one index. ``base`` is an n x dim uint8 or
     float32 array/tensor. ``nav_samples`` = 0 writes no pivot graph.
 
@@ -68,7 +68,7 @@ def build_index(base, out_dir: str, R: int, M: int = 32, alpha: float = 1.2, nav
         t3 = time.time()
         ids = sample_pivots(n, min(nav_samples, n))
         sub = x[torch.from_numpy(ids.astype(np.int64)).to(x.device)]
-        ng, ndeg, nmed = builder.build(sub, nav_R, alpha, seed=seed + 1)
+        ng, ndeg, nmed = builder.build(sub, nav_R, alpha, seed=seed + 1, L_build=nav_L_build)
         if int(ndeg.min()) < 3:
             raise RuntimeError("pivot graph has a node with fewer than 3 neighbours")
         nav = (ids, sub, ng, ndeg, nmed)

@@ -183,10 +183,19 @@ class Reference:
             self._screened = {key: np.nonzero(ok)[0]}
         return self._screened[key]
 
+    def max_L(self) -> int:
+        """Largest L whose walk kernel the reference can launch: it asks for
+        20 (L + R) bytes of dynamic shared memory (src/pure_mem.cu:140) and
+        never raises the 48 KB default, so a larger L fails to launch and
+        leaves the outputs untouched."""
+        return (48 * 1024) // 20 - int(self.screens[0].max_m0)
+
     def search(self, q: np.ndarray, k: int, L: int, threads: int = 0):
         """Runs the reference on the screened rows of q. Returns (rows, ids,
         dists, found, seconds): rows are the indices into q that ran, the
         outputs hold one row per entry of rows."""
+        if L > self.max_L():
+            raise ValueError(f"the reference kernel cannot launch at L={L} (largest L {self.max_L()})")
         q = np.ascontiguousarray(q, dtype=np.float32)
         rows = self.screen(q, k, L, threads)
         self.last_skipped = int(q.shape[0] - rows.size)
