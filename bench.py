@@ -446,11 +446,17 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
+# Workloads too large for a full ncu capture on the device use the capture of
+# their tenth-size twin (same generator, cluster density and graph shape).
+CAPTURE_CASE = {"c2": "c2_10m"}
+
+
 def traffic_per_hop(kernel: str, workload: str):
     """DRAM bytes per hop of `kernel` from a committed ncu capture of the same
-    workload (profiles/<kernel>_<workload>.json), if any. The bench scales it by
-    the hops it counted, since its calibrated L may differ from the capture's."""
-    p = ROOT / "profiles" / f"{kernel}_{workload}.json"
+    workload (profiles/<kernel>_<workload>.json), or of its capture case, if
+    any. The bench scales it by the hops it counted, since its calibrated L may
+    differ from the capture's."""
+    p = ROOT / "profiles" / f"{kernel}_{CAPTURE_CASE.get(workload, workload)}.json"
     if p.exists():
         d = json.loads(p.read_text())
         return d.get("dram_bytes_per_hop")
@@ -788,7 +794,8 @@ def _run_ours(args, rank, world, local):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak if peak else None,
                      "traffic": None if tph is None else tph * r["hops_per_query"] * nq,
-                     "traffic_source": "ncu capture scaled by counted hops (profiles/)" if tph else None,
+                     "traffic_source": (f"ncu capture of {CAPTURE_CASE.get(args.workload, args.workload)} "
+                                        "(profiles/), DRAM bytes per hop x counted hops") if tph else None,
                      "peak_kind": peak_kind,
                      "kernel": "batch_search_kernel" if head != "plain" else "plain_search_kernel"},
         "e2e": {"value": world / e2e_total, "unit": "queries/s", "h2d_bytes_per_step": h2d,

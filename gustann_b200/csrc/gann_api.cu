@@ -656,7 +656,7 @@ int gann_autotune(gann_t* h, const float* d_queries, int nq, int topk, int ef_se
     cudaStream_t s = h->stream;
     const int base_bits = gann::batch_hash_bits(ef_search);
     for (int W : {2, 4, 8}) {
-      for (int delta : {-1, 0, 1}) {
+      for (int delta : {-3, -2, -1, 0, 1}) {  // smaller caches trade re-scoring for CTAs per SM
         gann_batch_opts_t o{};
         o.precision = precision;
         o.beam_width = W;

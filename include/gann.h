@@ -172,7 +172,7 @@ int gann_search_batch_device(gann_t* h, const float* d_queries, int nq, const in
                              int32_t* d_found_cnt, int32_t* d_hops, int64_t* d_bytes, void* stream);
 
 /* Autotuner of the batched form: times beam widths {2, 4, 8} and visited
- * caches of {1/2, 1, 2} x the default size on nq device queries at (topk,
+ * caches of {1/8, 1/4, 1/2, 1, 2} x the default size on nq device queries at (topk,
  * ef_search, precision), keeps the fastest, and makes it this handle's default
  * for gann_search_batch* calls that leave beam_width / hash_bits at 0. Results
  * do not depend on the cache size; the beam width changes the walk order. The
