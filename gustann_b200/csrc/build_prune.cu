@@ -9,13 +9,16 @@
 //
 // One warp per row. The row's candidates (ids, -1 = none; duplicates, the point
 // itself and ids outside [0, n) are dropped) and the point's own vector are
-// staged in shared memory, one padded row each (an odd word stride, so lanes
-// reading different rows at the same word hit different banks). Each lane
-// scores its candidates against the point, the candidates are ranked by
-// (distance, id), and the keep/occlude pass walks them in that order; every
-// lane re-checks its own candidates against each kept one. uint8 vectors are
-// compared with byte-wise |a - b| and a 4-way dot product (exact in int32),
-// float vectors in FP32.
+// staged in shared memory, one padded row each. Each lane scores its
+// candidates against the point, the candidates are ranked by (distance, id),
+// and the keep/occlude pass walks them in that order; every lane re-checks its
+// own candidates against each kept one. uint8 vectors are compared with
+// byte-wise |a - b| and a 4-way dot product (exact in int32), rows at an odd
+// word stride so that lanes reading different rows at the same word hit
+// different banks. Float vectors of a dimension divisible by 4 are compared
+// as |a|^2 + |b|^2 - 2 a.b in FP32 with 16-byte shared-memory loads (rows at a
+// stride of dim + 4 words, norms computed once per row); other float rows by
+// their differences.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -41,14 +44,33 @@ struct PruneArgs {
   float alpha;
   int wpb;           // warps per block
   int warp_words;    // shared-memory words per warp
+  int vec4;          // float rows compared through norms and 16-byte loads
   int32_t* out;      // n_rows x R, -1 padded
 };
 
+// Squared L2 between two staged rows (na, nb: their squared norms, used by the
+// vec4 float form only).
 template <class T>
-__device__ __forceinline__ float row_dist(const uint32_t* a, const uint32_t* b, int words);
+__device__ __forceinline__ float row_dist(const uint32_t* a, const uint32_t* b, int words, float na, float nb,
+                                          bool vec4);
+
+// Squared norm of a staged float row (vec4 form).
+__device__ __forceinline__ float row_norm(const uint32_t* a, int words) {
+  const float4* x = reinterpret_cast<const float4*>(a);
+  float acc = 0.0f;
+  for (int w = 0; w < words / 4; w++) {
+    const float4 v = x[w];
+    acc = fmaf(v.x, v.x, acc);
+    acc = fmaf(v.y, v.y, acc);
+    acc = fmaf(v.z, v.z, acc);
+    acc = fmaf(v.w, v.w, acc);
+  }
+  return acc;
+}
 
 template <>
-__device__ __forceinline__ float row_dist<uint8_t>(const uint32_t* a, const uint32_t* b, int words) {
+__device__ __forceinline__ float row_dist<uint8_t>(const uint32_t* a, const uint32_t* b, int words, float, float,
+                                                   bool) {
   unsigned acc = 0;
   for (int w = 0; w < words; w++) {
     const unsigned d = __vabsdiffu4(a[w], b[w]);
@@ -58,7 +80,33 @@ __device__ __forceinline__ float row_dist<uint8_t>(const uint32_t* a, const uint
 }
 
 template <>
-__device__ __forceinline__ float row_dist<float>(const uint32_t* a, const uint32_t* b, int words) {
+__device__ __forceinline__ float row_dist<float>(const uint32_t* a, const uint32_t* b, int words, float na, float nb,
+                                                 bool vec4) {
+  if (vec4) {
+    const float4* x = reinterpret_cast<const float4*>(a);
+    const float4* y = reinterpret_cast<const float4*>(b);
+    float d0 = 0.0f, d1 = 0.0f;
+    int w = 0;
+    for (; w + 1 < words / 4; w += 2) {
+      const float4 p0 = x[w], q0 = y[w], p1 = x[w + 1], q1 = y[w + 1];
+      d0 = fmaf(p0.x, q0.x, d0);
+      d0 = fmaf(p0.y, q0.y, d0);
+      d0 = fmaf(p0.z, q0.z, d0);
+      d0 = fmaf(p0.w, q0.w, d0);
+      d1 = fmaf(p1.x, q1.x, d1);
+      d1 = fmaf(p1.y, q1.y, d1);
+      d1 = fmaf(p1.z, q1.z, d1);
+      d1 = fmaf(p1.w, q1.w, d1);
+    }
+    if (w < words / 4) {
+      const float4 p0 = x[w], q0 = y[w];
+      d0 = fmaf(p0.x, q0.x, d0);
+      d0 = fmaf(p0.y, q0.y, d0);
+      d0 = fmaf(p0.z, q0.z, d0);
+      d0 = fmaf(p0.w, q0.w, d0);
+    }
+    return fmaxf(na + nb - 2.0f * (d0 + d1), 0.0f);
+  }
   float acc = 0.0f;
   for (int w = 0; w < words; w++) {
     const float d = __uint_as_float(a[w]) - __uint_as_float(b[w]);
@@ -105,6 +153,8 @@ __global__ void __launch_bounds__(256) prune_kernel(PruneArgs a) {
   int32_t* order = reinterpret_cast<int32_t*>(vecs + (size_t)(K + 1) * a.stride);  // sorted -> slot
   float* sd = reinterpret_cast<float*>(order + kPruneMaxK);                         // sorted distances
   int32_t* sid = reinterpret_cast<int32_t*>(sd + kPruneMaxK);                       // sorted ids
+  float* nrm = reinterpret_cast<float*>(sid + kPruneMaxK);                          // row norms (vec4 form)
+  const bool vec4 = a.vec4 != 0;
   const int64_t p = a.rows ? (int64_t)__ldg(a.rows + row) : row;
   int32_t* out = a.out + row * R;
   if (p < 0 || p >= a.n) {  // no such point: an empty row
@@ -125,11 +175,21 @@ __global__ void __launch_bounds__(256) prune_kernel(PruneArgs a) {
     if (cv[t]) stage_row<T>(a, cid[t], vecs + (size_t)(lane + 32 * t) * a.stride);
   if (lane == (K & 31)) stage_row<T>(a, p, vecs + (size_t)K * a.stride);
   __syncwarp();
+  if (vec4) {
+#pragma unroll
+    for (int t = 0; t < KP; t++)
+      if (cv[t]) nrm[lane + 32 * t] = row_norm(vecs + (size_t)(lane + 32 * t) * a.stride, a.row_words);
+    if (lane == (K & 31)) nrm[K] = row_norm(vecs + (size_t)K * a.stride, a.row_words);
+    __syncwarp();
+  }
   const uint32_t* vp = vecs + (size_t)K * a.stride;
+  const float np_ = vec4 ? nrm[K] : 0.0f;
   float d[KP];
 #pragma unroll
   for (int t = 0; t < KP; t++)
-    d[t] = cv[t] ? row_dist<T>(vecs + (size_t)(lane + 32 * t) * a.stride, vp, a.row_words) : __int_as_float(0x7f800000);
+    d[t] = cv[t] ? row_dist<T>(vecs + (size_t)(lane + 32 * t) * a.stride, vp, a.row_words,
+                               vec4 ? nrm[lane + 32 * t] : 0.0f, np_, vec4)
+                 : __int_as_float(0x7f800000);
   // rank by (distance, id, slot): a repeated id gets consecutive ranks
   int rank[KP];
 #pragma unroll
@@ -180,11 +240,14 @@ __global__ void __launch_bounds__(256) prune_kernel(PruneArgs a) {
     count++;
     if (count == R) break;
     const uint32_t* vj = vecs + (size_t)order[j] * a.stride;
+    const float nj = vec4 ? nrm[order[j]] : 0.0f;
 #pragma unroll
     for (int t = 0; t < KP; t++) {
       const int pos = lane + 32 * t;
       if (al[t] && pos > j) {
-        const float djc = row_dist<T>(vj, vecs + (size_t)order[pos] * a.stride, a.row_words);
+        const int oc = order[pos];
+        const float djc = row_dist<T>(vj, vecs + (size_t)oc * a.stride, a.row_words, nj, vec4 ? nrm[oc] : 0.0f,
+                                      vec4);
         if (a.alpha * djc < sd[pos]) al[t] = false;
       }
     }
@@ -241,14 +304,15 @@ extern "C" int gann_build_prune(const void* d_x, int dtype, int64_t n, int dim, 
   a.n = n;
   a.dim = dim;
   a.row_words = dtype == GANN_UINT8 ? (dim + 3) / 4 : dim;
-  a.stride = a.row_words | 1;
+  a.vec4 = dtype == GANN_FLOAT && dim % 4 == 0;
+  a.stride = a.vec4 ? dim + 4 : (a.row_words | 1);  // 16-byte rows for the vec4 form, else an odd stride
   a.rows = d_rows;
   a.cand = d_cand;
   a.n_rows = n_rows;
   a.K = K;
   a.R = R;
   a.alpha = alpha;
-  a.warp_words = (K + 1) * a.stride + 3 * kPruneMaxK;
+  a.warp_words = (K + 1) * a.stride + 3 * kPruneMaxK + 4 * ((kPruneMaxK + 1 + 3) / 4);  // + norms; a multiple of 4
   a.out = d_out;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const cudaError_t e = dtype == GANN_UINT8 ? launch_prune_t<uint8_t>(a, s) : launch_prune_t<float>(a, s);

@@ -435,7 +435,8 @@ int enqueue_batch(gann_t* h, const float* d_q, int nq, const int32_t* d_k, const
   if (opts) o = *opts;
   const int prec = opts ? o.precision : GANN_PREC_BF16X3;
   const int W = o.beam_width ? o.beam_width : (h->tuned_beam ? h->tuned_beam : 4);
-  if (!(W == 1 || W == 2 || W == 4 || W == 8)) return set_error(GANN_EINVAL, "beam_width must be 1, 2, 4 or 8");
+  if (!(W == 1 || W == 2 || W == 4 || W == 8 || W == 16))
+    return set_error(GANN_EINVAL, "beam_width must be 1, 2, 4, 8 or 16");
   if (prec < GANN_PREC_FP32 || prec > GANN_PREC_BF16_CC) return set_error(GANN_EINVAL, "unknown precision");
   const int hb = o.hash_bits ? o.hash_bits : gann::batch_hash_bits(l_max) + h->tuned_hash_delta;
   if (hb < 4 || hb > 16) return set_error(GANN_EINVAL, "hash_bits must be in 4..16");
@@ -655,7 +656,7 @@ int gann_autotune(gann_t* h, const float* d_queries, int nq, int topk, int ef_se
     std::lock_guard<std::mutex> lk(h->mu);
     cudaStream_t s = h->stream;
     const int base_bits = gann::batch_hash_bits(ef_search);
-    for (int W : {2, 4, 8}) {
+    for (int W : {2, 4, 8, 16}) {
       for (int delta : {-3, -2, -1, 0, 1}) {  // smaller caches trade re-scoring for CTAs per SM
         gann_batch_opts_t o{};
         o.precision = precision;

@@ -62,7 +62,8 @@ extern "C" int gann_search_batch_noalloc(gann_t* h, const float* d_queries, int 
   // The same defaults as gann_search_batch_device: the handle's tuned beam
   // width and visited-cache delta (gann_autotune) when the options leave 0.
   const int W = o.beam_width ? o.beam_width : (h->tuned_beam ? h->tuned_beam : 4);
-  if (!(W == 1 || W == 2 || W == 4 || W == 8)) return gann_internal_set_error(GANN_EINVAL, "beam_width must be 1, 2, 4 or 8");
+  if (!(W == 1 || W == 2 || W == 4 || W == 8 || W == 16))
+    return gann_internal_set_error(GANN_EINVAL, "beam_width must be 1, 2, 4, 8 or 16");
   if (prec < GANN_PREC_FP32 || prec > GANN_PREC_BF16_CC) return gann_internal_set_error(GANN_EINVAL, "unknown precision");
   const bool tc = prec == GANN_PREC_BF16 || prec == GANN_PREC_BF16X3;
   if (tc && nq > kNoAllocMaxQueries)

@@ -333,7 +333,7 @@ struct Record {
 };
 
 template <class T, class TabT, int W, bool PK>
-__global__ void __launch_bounds__(W * 32, 24 / W) batch_search_kernel(BatchParams p) {
+__global__ void __launch_bounds__(W * 32, W <= 8 ? 24 / W : 1) batch_search_kernel(BatchParams p) {
   constexpr int NT = W * 32;
   constexpr int TKW = W - 1;  // warp that marks the picks and keeps the top-k
   extern __shared__ __align__(16) uint8_t smem[];
@@ -756,6 +756,7 @@ cudaError_t launch_t(const BatchParams& p, int W, int num_sms, cudaStream_t stre
     case 2: return launch_w<T, TabT, 2>(p, num_sms, stream);
     case 4: return launch_w<T, TabT, 4>(p, num_sms, stream);
     case 8: return launch_w<T, TabT, 8>(p, num_sms, stream);
+    case 16: return launch_w<T, TabT, 16>(p, num_sms, stream);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -64,7 +64,7 @@ enum {
  * up to 2^-5 of a chunk's range to cancellation in |r|^2 - 2 r.P + |P|^2). */
 typedef struct {
   int32_t precision;   /* GANN_PREC_*; opts = NULL means GANN_PREC_BF16X3 */
-  int32_t beam_width;  /* warps (nodes expanded per step) per query: 1, 2, 4 or 8; 0 = 4 */
+  int32_t beam_width;  /* warps (nodes expanded per step) per query: 1, 2, 4, 8 or 16; 0 = 4 (or autotuned) */
   int32_t hash_bits;   /* visited cache of 2^hash_bits ids per query; 0 = sized from L */
   int32_t reserved[5];
 } gann_batch_opts_t;
@@ -171,7 +171,7 @@ int gann_search_batch_device(gann_t* h, const float* d_queries, int nq, const in
                              const gann_batch_opts_t* opts, int32_t* d_nns, float* d_distances,
                              int32_t* d_found_cnt, int32_t* d_hops, int64_t* d_bytes, void* stream);
 
-/* Autotuner of the batched form: times beam widths {2, 4, 8} and visited
+/* Autotuner of the batched form: times beam widths {2, 4, 8, 16} and visited
  * caches of {1/8, 1/4, 1/2, 1, 2} x the default size on nq device queries at (topk,
  * ef_search, precision), keeps the fastest, and makes it this handle's default
  * for gann_search_batch* calls that leave beam_width / hash_bits at 0. Results

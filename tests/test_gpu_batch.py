@@ -255,7 +255,7 @@ def test_batched_fp32_matches_cpu_model(golden, oracle_mod, name):
     model = BatchModel(oracle_mod, meta)
     g = open_meta(meta)
     q = meta["queries"][:100]
-    for k, L, W, hb in ((10, 40, 4, 4), (10, 24, 1, 4), (5, 32, 2, 5), (10, 64, 8, 4)):
+    for k, L, W, hb in ((10, 40, 4, 4), (10, 24, 1, 4), (5, 32, 2, 5), (10, 64, 8, 4), (10, 96, 16, 5)):
         ids, dis, fnd, _ = g.search_batch(q, k, L, precision=gb.PREC_FP32, beam_width=W, hash_bits=hb)
         mi, md, mf = model.search(q, k, L, W)
         what = f"{name} k={k} L={L} W={W} hash_bits={hb}"
