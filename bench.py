@@ -45,10 +45,15 @@ WORKLOADS = {
     "small": ("u8", 100_000, 128, 100, 64, 32, 1_000),
     "c0": ("u8", 1_000_000, 128, 1_000, 64, 32, 10_000),
     "c1": ("f32", 10_000_000, 96, 4_096, 64, 32, 100_000),
-    "c2": ("u8", 100_000_000, 128, 10_000, 32, 32, 1_000_000),
+    "c2": ("u8", 100_000_000, 128, 10_000, 32, 32, 100_000),
     # the C2 generator and graph shape at a tenth of the size (10,000 points per cluster as in c2)
     "c2_10m": ("u8", 10_000_000, 128, 1_000, 32, 32, 100_000),
 }
+# Partitioned builds: the sample whose pivot graph supplies the main graph's
+# long edges (1% of the points), when the entry file is sparser. At 100M a 0.1%
+# entry file (10 pivots per cluster of the mixture) lets the entry walk route
+# between clusters; a 1% file (100 per cluster) mostly does not.
+EMBED_SAMPLES = {"c2": 1_000_000}
 L_LADDER = [16, 24, 32, 48, 64, 96, 128, 160, 192, 256, 320, 384, 448, 512, 640, 768, 1024, 1536, 2048, 3072, 4096]
 MIX_L, MIX_K = (32, 64, 128, 256), (1, 10, 100)
 
@@ -118,14 +123,16 @@ def build_workload(workload: str, nq: int, cache: Path) -> None:
     t0 = time.time()
     base, qs = synth.make(kind, n, dim, clusters, nq, backend="torch", device="cuda")
     log(f"{workload}: data generated in {time.time() - t0:.1f} s")
-    f = build_index(base, str(d), R=R, M=M, nav_samples=nav, device="cuda", log=log)
+    f = build_index(base, str(d), R=R, M=M, nav_samples=nav, device="cuda", log=log,
+                    embed_samples=EMBED_SAMPLES.get(workload))
     t1 = time.time()
     gt = groundtruth.knn(base, qs, 100)
     log(f"{workload}: ground truth in {time.time() - t1:.1f} s")
     np.save(d / "queries.npy", qs.float().cpu().numpy())
     np.save(d / "gt.npy", gt)
     meta = {"workload": workload, "kind": kind, "n": n, "dim": dim, "clusters": clusters, "R": R, "M": M,
-            "nav": nav, "nq": nq, "index_file": f.index_file, "pq_prefix": f.pq_prefix,
+            "nav": nav, "embed": EMBED_SAMPLES.get(workload, nav), "nq": nq, "index_file": f.index_file,
+            "pq_prefix": f.pq_prefix,
             "nav_dir": f.nav_dir, "build_s": time.time() - t0, "timings": f.timings}
     (d / "ready.json").write_text(json.dumps(meta))
 
@@ -155,7 +162,8 @@ def config_of(meta: dict, nq: int, k: int) -> dict:
     gb = (meta["n"] * (meta["dim"] * (1 if meta["kind"] == "u8" else 4) + 4 * (meta["R"] + 1)) * 1.0
           + meta["n"] * meta["M"]) / 1e9
     return {"workload": meta["workload"], "n": meta["n"], "dim": meta["dim"], "vector": meta["kind"],
-            "R": meta["R"], "pq_chunks": meta["M"], "nav_points": meta["nav"], "queries_per_step": nq, "k": k,
+            "R": meta["R"], "pq_chunks": meta["M"], "nav_points": meta["nav"],
+            "embedded_pivot_points": meta.get("embed", meta["nav"]), "queries_per_step": nq, "k": k,
             "recall_target": 0.95,
             "l2": f"inputs larger than L2: records + codes {gb:.1f} GB, gathered at random"}
 

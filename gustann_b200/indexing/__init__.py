@@ -43,9 +43,17 @@ def _np(x):
 def build_index(base, out_dir: str, R: int, M: int = 32, alpha: float = 1.2, nav_samples: int | None = None,
                 nav_R: int = 32, device=None, n_coarse: int | None = None, nprobe: int = 4,
                 pq_train: int = 1 << 18, seed: int = 7, legacy_pq: bool = False, method: str = "auto",
-                leaf: int = 4096, nav_L_build: int = 100, log=None) -> IndexFiles:
+                leaf: int = 4096, nav_L_build: int = 100, embed_samples: int | None = None,
+                log=None) -> IndexFiles:
     """Build and write every file of one index. ``base`` is an n x dim uint8 or
     float32 array/tensor. ``nav_samples`` = 0 writes no pivot graph.
+
+    ``embed_samples`` (partitioned builder only): the sample whose pivot graph
+    supplies the main graph's long edges, when it should differ from the entry
+    file's. A sparser entry file routes the entry walk (a beam of 4,
+    src/impl/nav.cuh:11-12) better across many clusters, while a denser
+    embedded sample gives more nodes long edges; both samples are prefixes of
+    the same shuffle, so the entry file's points are embedded points too.
 
     ``method``: "vamana" (builder.build: Vamana searches from the medoid),
     "ivf" (ivf.build: exact leaf neighbourhoods, pruned, reverse edges, the
@@ -75,13 +83,25 @@ def build_index(base, out_dir: str, R: int, M: int = 32, alpha: float = 1.2, nav
         timings["nav_s"] = time.time() - t3
         if log:
             log(f"pivot graph: {len(ids)} points, {timings['nav_s']:.1f} s")
+    embed = (nav[0], nav[2]) if nav else None
+    if large and embed_samples and nav and embed_samples != len(nav[0]):
+        t3 = time.time()
+        eids = sample_pivots(n, min(embed_samples, n))
+        esub = x[torch.from_numpy(eids.astype(np.int64)).to(x.device)]
+        eg, _, _ = builder.build(esub, nav_R, alpha, seed=seed + 1, L_build=nav_L_build)
+        embed = (eids, eg)
+        del esub
+        timings["embed_pivots_s"] = time.time() - t3
+        if log:
+            log(f"embedded pivot graph: {len(eids)} points, {timings['embed_pivots_s']:.1f} s")
     t1 = time.time()
     index_file = os.path.join(out_dir, "index_disk.index")
     if large:
         from . import ivf
 
         g, deg, med, gt = ivf.build(x, R, alpha, seed=seed, leaf=leaf,
-                                    pivots=nav[0] if nav else None, nav_graph=nav[2] if nav else None, log=log)
+                                    pivots=embed[0] if embed else None, nav_graph=embed[1] if embed else None,
+                                    log=log)
         timings.update({f"graph_{k}": v for k, v in gt.items()})
         timings["graph_s"] = time.time() - t1
         t2 = time.time()

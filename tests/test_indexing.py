@@ -217,3 +217,22 @@ def test_embedded_pivot_edges_are_the_far_end_of_the_pivot_rows():
     out = ivf.embed_pivots(g.clone(), piv, nav, 2)
     assert out[2].tolist() == [108, 109, 5, -1]  # kept 2 nearest, then pivot 1 (= node 5); its own id is dropped
     assert out[5].tolist() == [120, 121, 2, -1]
+
+
+def test_sparser_entry_file_than_embedded_pivots(tmp_path, oracle_mod):
+    """embed_samples: the entry file holds the first 150 points of the pivot
+    shuffle while the main graph embeds the 600-point pivot graph's long
+    edges; the files stay valid and searchable."""
+    from gustann_b200 import sample_pivots
+
+    base, qs = synth.make("u8", 6000, 32, 12, 60, backend="numpy")
+    f = build_index(base, str(tmp_path), R=16, M=8, nav_samples=150, embed_samples=600, method="ivf", leaf=512)
+    assert "embed_pivots_s" in f.timings
+    mapping = np.loadtxt(f"{f.nav_dir}/map.txt", dtype=np.int64)
+    np.testing.assert_array_equal(mapping, sample_pivots(6000, 150))
+    assert set(mapping.tolist()) <= set(sample_pivots(6000, 600).tolist())  # nested samples
+    gt = groundtruth.knn(torch.from_numpy(base), torch.from_numpy(qs), 10)
+    o = oracle_mod.Oracle(f.index_file, f.pq_prefix, f.nav_dir, 0)
+    ids, *_, flags, _ = o.search(qs.astype(np.float32), 10, 64)
+    assert not flags.any()
+    assert groundtruth.recall(ids, gt, 10) > 0.9
