@@ -893,7 +893,8 @@ def run_reference(args, rank, world, local):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(secs) / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic seeded Gaussian mixture; same index files as the GPU arm",
-        "config": config_of(meta, sample, k),
+        # the workload both arms run; each timed step here is a bounded sample of it
+        "config": config_of(meta, nq, k), "sample_queries_per_step": sample,
         "form": "reference algorithm on host cores", "L": L, "calibration_s": cal_s,
         "recall": calc_recall(ids, gt[:sample], k), "recall_all_queries": rec_cal,
         "cpu_baseline": {"value": value, "unit": "queries/s", "cores": cores, "kind": "port",
