@@ -149,48 +149,31 @@ __device__ __forceinline__ float adc32_words(const TabT* table, const uint4& a, 
 // into the sorted top-k (td, ti, size) in one pass of one warp. Pairs with an
 // infinite distance are skipped. The result equals n calls of topk_push in
 // order: a new pair goes after existing entries with an equal distance, and
-// after earlier new pairs with an equal distance.
+// after earlier new pairs with an equal distance. Lane j holds pair j; the
+// others' distances come by shuffle, so no per-pair registers are held.
 template <int N>
 __device__ __forceinline__ void topk_push_many(float* td, int32_t* ti, int& size, int k, const float* vd,
                                                const int32_t* vi, int n, int lane) {
-  float cd[N];
-  bool cv[N];
-#pragma unroll
-  for (int j = 0; j < N; j++) {
-    cd[j] = j < n ? vd[j] : inf_f();
-    cv[j] = j < n && cd[j] != inf_f();
-  }
-  int nv = 0;
-#pragma unroll
-  for (int j = 0; j < N; j++) nv += cv[j];
+  const bool mine = lane < N && lane < n && vd[lane] != inf_f();
+  const float my_d = mine ? vd[lane] : inf_f();
+  const int32_t my_id = mine ? vi[lane] : 0;
+  const unsigned vm = __ballot_sync(kFull, mine);
+  const int nv = __popc(vm);
   if (nv == 0) return;
-  if (size == k) {  // full: only a pair below the k-th distance can enter
-    const float worst = td[k - 1];
-    bool any = false;
-#pragma unroll
-    for (int j = 0; j < N; j++) any |= cv[j] && cd[j] < worst;
-    if (!any) return;
-  }
-  float my_d = inf_f();
-  int32_t my_id = 0;
-  bool mine = false;
-  int pos = 0;  // final position of pair `lane` (lane < n)
+  if (size == k && !__ballot_sync(kFull, mine && my_d < td[k - 1])) return;  // full: must beat the k-th
+  int pos = 0;  // final position of pair `lane`
 #pragma unroll
   for (int j = 0; j < N; j++) {
-    if (lane == j && cv[j]) {
-      mine = true;
-      my_d = cd[j];
-      my_id = vi[j];
-    }
+    const float dj = __shfl_sync(kFull, my_d, j);
+    pos += ((vm >> j) & 1u) && (dj < my_d || (dj == my_d && j < lane));
   }
-#pragma unroll
-  for (int j = 0; j < N; j++) pos += cv[j] && (cd[j] < my_d || (cd[j] == my_d && j < lane));
   for (int base = 0; base < size; base += 32) {
     const int i = base + lane;
     const float e = i < size ? td[i] : inf_f();
 #pragma unroll
     for (int j = 0; j < N; j++) {
-      const int c = __popc(__ballot_sync(kFull, i < size && e <= cd[j]));
+      const float dj = __shfl_sync(kFull, my_d, j);  // every lane takes part in the shuffle
+      const int c = __popc(__ballot_sync(kFull, i < size && e <= dj));
       if (lane == j) pos += c;
     }
   }
@@ -198,14 +181,13 @@ __device__ __forceinline__ void topk_push_many(float* td, int32_t* ti, int& size
   if (__ballot_sync(kFull, enters)) {
     for (int c = (size - 1) >> 5; c >= 0; c--) {  // existing entries move up, top chunk first
       const int i = c * 32 + lane;
-      float e = 0.0f;
-      int32_t eid = 0;
+      const float e = i < size ? td[i] : 0.0f;
+      const int32_t eid = i < size ? ti[i] : 0;
       int sh = 0;
-      if (i < size) {
-        e = td[i];
-        eid = ti[i];
 #pragma unroll
-        for (int j = 0; j < N; j++) sh += cv[j] && cd[j] < e;
+      for (int j = 0; j < N; j++) {
+        const float dj = __shfl_sync(kFull, my_d, j);
+        sh += ((vm >> j) & 1u) && dj < e;
       }
       __syncwarp();
       if (i < size && i + sh < k) {
@@ -298,7 +280,9 @@ __device__ void copy_table(void* dst, const __nv_bfloat16* src, int bytes, int t
   for (int i = tid; i < bytes / 16; i += nthreads) d[i] = __ldg(s + i);
 }
 
-constexpr int kStage = 4;  // list entries per thread staged in registers by the in-place merge
+// List entries per thread staged in registers by the in-place merge: 1,024
+// entries per round for W >= 8.
+__host__ __device__ constexpr int stage_per_thread(int W) { return W >= 16 ? 2 : 4; }
 
 // The node's record as one warp holds it: degree, the first kEdgeRegs * 32
 // neighbour slots and kVecRegs * 32 vector elements, loaded in one round trip.
@@ -333,7 +317,7 @@ struct Record {
 };
 
 template <class T, class TabT, int W, bool PK>
-__global__ void __launch_bounds__(W * 32, W <= 8 ? 24 / W : 1) batch_search_kernel(BatchParams p) {
+__global__ void __launch_bounds__(W * 32, W <= 8 ? 24 / W : 2) batch_search_kernel(BatchParams p) {
   constexpr int NT = W * 32;
   constexpr int TKW = W - 1;  // warp that marks the picks and keeps the top-k
   extern __shared__ __align__(16) uint8_t smem[];
@@ -406,17 +390,21 @@ __global__ void __launch_bounds__(W * 32, W <= 8 ? 24 / W : 1) batch_search_kern
     // when the step starts: the first step picks the entry, and each step
     // works out the next step's picks from the sorted survivors before it
     // rewrites the list, so that each warp's next record is already on its
-    // way while the list is merged.
+    // way while the list is merged. Lane w of warp 0 holds the list position
+    // of pick w and marks it expanded when the step starts, after the merge
+    // that placed it; every comparison of the step masks the mark off, and the
+    // scan for old candidates starts after the last pick, so that write
+    // changes nothing the step reads before barrier (1), which orders it
+    // before the merge reads the list.
     int sz = u0 >= 0 ? 1 : 0, found = 0, hops = 0;
     int npick = u0 >= 0 ? 1 : 0, last_pos = 0;
-    int pick_pos[W];
-#pragma unroll
-    for (int w = 0; w < W; w++) pick_pos[w] = w == 0 && u0 >= 0 ? 0 : -1;
+    int my_pick = 0;  // warp 0, lane w < npick: position of pick w
     Record<T, PK> rec;
     if (warp == 0 && u0 >= 0) rec.load(p, u0, lane);
 
     for (;;) {
       if (npick == 0 || s.ctrl[6]) break;
+      if (warp == 0 && lane < npick) list_id[my_pick] |= kExpanded;
       const bool full = sz == L;
       const float tail_d = full ? list_d[L - 1] : 0.0f;
       const uint32_t tail_id = full ? list_id[L - 1] : 0u;
@@ -519,13 +507,7 @@ __global__ void __launch_bounds__(W * 32, W <= 8 ? 24 / W : 1) batch_search_kern
       __syncthreads();  // (1) survivors and exact distances are in
       const int nsv = s.ctrl[2];
       const int first_new = s.ctrl[7];  // INT_MAX when nothing survived
-      // The merge's first round covers [lo1, sz); a pick there is marked when
-      // it is staged, every other pick in place.
-      const int lo1 = min(sz, max(first_new, sz - kStage * NT));
-      if (warp == TKW) {  // mark the picks outside the first round, keep the top-k
-#pragma unroll
-        for (int w = 0; w < W; w++)
-          if (lane == w && w < npick && pick_pos[w] < lo1) list_id[pick_pos[w]] |= kExpanded;
+      if (warp == TKW) {  // keep the top-k
         topk_push_many<W>(s.topk_d, s.topk_id, found, k, s.sel_d, s.sel_id, npick, lane);
         hops += npick;
         if (lane == 0 && hops > kHopCap) {
@@ -559,31 +541,26 @@ __global__ void __launch_bounds__(W * 32, W <= 8 ? 24 / W : 1) batch_search_kern
       // In-place merge. Entries from the first insertion point on move up:
       // old entry i goes to i + #{survivors inserted at or before i}, survivor
       // r to its insertion point + r; positions >= L drop. Each round stages
-      // the top kStage * NT entries still to move in registers, waits for
-      // every thread, then writes; the first round's wait is barrier (2)
-      // (a pick staged there takes its expanded mark with it), and survivors
-      // are written after the last round.
-      uint32_t st_id[kStage];
-      float st_d[kStage];
+      // the top KS * NT entries still to move in registers, waits for
+      // every thread, then writes; the first round's wait is barrier (2), and
+      // survivors are written after the last round.
+      constexpr int KS = stage_per_thread(W);
+      uint32_t st_id[KS];
+      float st_d[KS];
       int hi = sz;
-      auto round_lo = [&]() { return min(hi, max(first_new, hi - kStage * NT)); };
-      auto stage = [&](bool first) {
+      auto round_lo = [&]() { return min(hi, max(first_new, hi - KS * NT)); };
+      auto stage = [&]() {
         const int lo = round_lo();
 #pragma unroll
-        for (int r = 0; r < kStage; r++) {
+        for (int r = 0; r < KS; r++) {
           const int i = lo + r * NT + tid;
           if (i < hi) {
-            uint32_t id = list_id[i];
-            if (first) {
-#pragma unroll
-              for (int w = 0; w < W; w++) id |= pick_pos[w] == i ? kExpanded : 0u;
-            }
-            st_id[r] = id;
+            st_id[r] = list_id[i];
             st_d[r] = list_d[i];
           }
         }
       };
-      stage(true);
+      stage();
       __syncthreads();  // (2)
       uint32_t* const sid = s.c_id;
       int ns = nsv;
@@ -650,7 +627,7 @@ __global__ void __launch_bounds__(W * 32, W <= 8 ? 24 / W : 1) batch_search_kern
           const int srcl = sel ? __ffs(sel) - 1 : 0;
           const int ppos = __shfl_sync(kFull, mpos, srcl);
           const uint32_t pid = __shfl_sync(kFull, mid, srcl);
-          pick_pos[w] = sel ? ppos : -1;
+          if (lane == w) my_pick = ppos;
           if (sel) last_pos = ppos;
           if (w == warp) my_next = pid;
         }
@@ -660,7 +637,7 @@ __global__ void __launch_bounds__(W * 32, W <= 8 ? 24 / W : 1) batch_search_kern
         for (;;) {
           const int lo = round_lo();
 #pragma unroll
-          for (int r = 0; r < kStage; r++) {
+          for (int r = 0; r < KS; r++) {
             const int i = lo + r * NT + tid;
             if (i < hi) {
               int a = 0, b = ns;
@@ -677,7 +654,7 @@ __global__ void __launch_bounds__(W * 32, W <= 8 ? 24 / W : 1) batch_search_kern
           }
           hi = lo;
           if (hi <= first_new) break;
-          stage(false);
+          stage();
           __syncthreads();
         }
         // Every old entry was read before a barrier that precedes this point,

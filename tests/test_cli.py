@@ -21,7 +21,7 @@ def cli():
 
 
 def run(args):
-    return subprocess.run([cli()] + [str(x) for x in args], capture_output=True, text=True, timeout=600)
+    return subprocess.run([cli()] + [str(x) for x in args], capture_output=True, text=True, timeout=300)
 
 
 def test_cli_argument_errors(tmp_path):
