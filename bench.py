@@ -54,6 +54,10 @@ WORKLOADS = {
 # entry file (10 pivots per cluster of the mixture) lets the entry walk route
 # between clusters; a 1% file (100 per cluster) mostly does not.
 EMBED_SAMPLES = {"c2": 1_000_000}
+# Entry node of the batched forms: 1 = the nearest point of the pivot file,
+# found for the whole batch on the tensor cores (gann_nearest_pivots), 0 = the
+# reference's beam-4 walk over the pivot graph. Set by --entry.
+ENTRY = 1
 L_LADDER = [16, 24, 32, 48, 64, 96, 128, 160, 192, 256, 320, 384, 448, 512, 640, 768, 1024, 1536, 2048, 3072, 4096]
 MIX_L, MIX_K = (32, 64, 128, 256), (1, 10, 100)
 
@@ -302,14 +306,17 @@ class PlainRunner:
 
 
 class BatchRunner(PlainRunner):
-    """gann_search_batch_device: W nodes per step, visited cache, BF16/FP32 tables."""
+    """gann_search_batch_device: W nodes per step, visited cache, BF16/FP32 tables,
+    the entry node from the pivot-graph walk or the nearest pivot (ENTRY)."""
 
-    def __init__(self, g, q_dev, k, precision, beam_width, name):
+    def __init__(self, g, q_dev, k, precision, beam_width, name, entry=None):
         super().__init__(g, q_dev, k)
         self.precision, self.W, self.name = precision, beam_width, name
+        self.entry = ENTRY if entry is None else entry
         import gustann_b200 as gb
 
-        self.launches_per_step = 2 if precision in (gb.PREC_BF16, gb.PREC_BF16X3) else 1
+        self.launches_per_step = (2 if precision in (gb.PREC_BF16, gb.PREC_BF16X3) else 1) + \
+            (1 if self.entry == gb.ENTRY_NEAREST_PIVOT else 0)
 
     def run(self, L, counters=False):
         import torch
@@ -318,7 +325,7 @@ class BatchRunner(PlainRunner):
         self.g.search_batch_device(self.q.data_ptr(), self.nq, 0, 0, self.k, L, self.ids.data_ptr(),
                                    self.dis.data_ptr(), self.fnd.data_ptr(),
                                    self.hops.data_ptr() if counters else 0, self.bytes.data_ptr() if counters else 0,
-                                   precision=self.precision, beam_width=self.W, stream=s)
+                                   precision=self.precision, beam_width=self.W, stream=s, entry=self.entry)
 
     def host_call(self, q_pinned, L, outs, t):
         import ctypes
@@ -326,7 +333,7 @@ class BatchRunner(PlainRunner):
         import gustann_b200 as gb
 
         ids, dis, fnd = outs
-        o = gb.GustANN._opts(self.precision, self.W, 0)
+        o = gb.GustANN._opts(self.precision, self.W, 0, self.entry)
         gb._check(gb.lib().gann_search_batch(self.g.handle, q_pinned.data_ptr(), self.nq, None, None, self.k, L,
                                              ctypes.byref(o), ids.data_ptr(), dis.data_ptr(), fnd.data_ptr(),
                                              ctypes.byref(t)))
@@ -403,11 +410,12 @@ def serving_sweep(g, meta, rates, seconds, max_batch, streams):
     Ls = np.exp(rng.uniform(np.log(32), np.log(512), len(q))).astype(np.int32)
     # admission budget: every request slot at a request of (k 10, L 256), so a
     # pipeline full of long-list requests refuses them before short ones
-    probe = gb.Server(g, max_batch=max_batch, streams=streams, topk_max=100, ef_max=512, precision=gb.PREC_BF16X3)
+    probe = gb.Server(g, max_batch=max_batch, streams=streams, topk_max=100, ef_max=512, precision=gb.PREC_BF16X3,
+                      entry=ENTRY)
     budget_kib = max_batch * (streams + 1) * probe.request_bytes(10, 256) // 1024
     probe.stop()
     srv = gb.Server(g, max_batch=max_batch, streams=streams, topk_max=100, ef_max=512, precision=gb.PREC_BF16X3,
-                    mem_budget_kib=budget_kib)
+                    mem_budget_kib=budget_kib, entry=ENTRY)
     out = []
     try:
         srv.open_loop(q, rates[0], 0.2, topk=ks, ef_search=Ls, seed=99)  # warm-up
@@ -512,7 +520,7 @@ class MixRunner:
         import torch
 
         self.g, self.q, self.name, self.plain = g, q_dev, name, plain
-        self.precision, self.W = precision, beam_width
+        self.precision, self.W, self.entry = precision, beam_width, ENTRY
         self.nq = q_dev.shape[0]
         self.kq, self.Lq = kq, Lq
         self.k_max, self.L_max = int(kq.max()), int(Lq.max())
@@ -536,7 +544,8 @@ class MixRunner:
             self.fnd = torch.zeros(self.nq, dtype=torch.int32, device="cuda")
             import gustann_b200 as gb
 
-            self.launches_per_step = 2 if precision in (gb.PREC_BF16, gb.PREC_BF16X3) else 1
+            self.launches_per_step = (2 if precision in (gb.PREC_BF16, gb.PREC_BF16X3) else 1) + \
+                (1 if self.entry == gb.ENTRY_NEAREST_PIVOT else 0)
 
     def run(self, L=None, counters=False):
         import torch
@@ -549,7 +558,8 @@ class MixRunner:
         else:
             self.g.search_batch_device(self.q.data_ptr(), self.nq, self.d_k.data_ptr(), self.d_L.data_ptr(),
                                        self.k_max, self.L_max, self.ids.data_ptr(), self.dis.data_ptr(),
-                                       self.fnd.data_ptr(), precision=self.precision, beam_width=self.W, stream=s)
+                                       self.fnd.data_ptr(), precision=self.precision, beam_width=self.W, stream=s,
+                                       entry=self.entry)
 
     def recall_by_k(self, gt) -> dict:
         ids = np.zeros((self.nq, self.k_max), np.int32)
@@ -722,16 +732,22 @@ def _run_ours(args, rank, world, local):
     t_open = time.time()
     g.init_pure_mem(gb.GustANNConfig(meta["index_file"], meta["pq_prefix"], meta["nav_dir"] or ""))
     open_s = time.time() - t_open
+    global ENTRY
+    if not g.info()["has_nav"]:
+        ENTRY = gb.ENTRY_NAV_WALK  # no pivot file: the walk starts at the medoid
     q = torch.from_numpy(meta["queries"]).cuda()
     gt = meta["gt"]
     k = args.k
     runners = {"plain": PlainRunner(g, q, k),
                "batched_bf16": BatchRunner(g, q, k, gb.PREC_BF16, args.beam, "batched_bf16"),
                "batched_bf16x3": BatchRunner(g, q, k, gb.PREC_BF16X3, args.beam, "batched_bf16x3"),
-               "batched_fp32": BatchRunner(g, q, k, gb.PREC_FP32, args.beam, "batched_fp32")}
-    forms_arg = args.forms or ("plain,batched_bf16,batched_bf16x3,batched_fp32" if meta["n"] > 2_000_000 else
-                               "plain,batched_bf16,batched_bf16x3,batched_fp32,host_plain,host_batched_bf16,"
-                               "host_batched_bf16_cached")
+               "batched_fp32": BatchRunner(g, q, k, gb.PREC_FP32, args.beam, "batched_fp32"),
+               "batched_bf16x3_walk": BatchRunner(g, q, k, gb.PREC_BF16X3, args.beam, "batched_bf16x3_walk",
+                                                  entry=gb.ENTRY_NAV_WALK)}
+    forms_arg = args.forms or ("plain,batched_bf16,batched_bf16x3,batched_fp32,batched_bf16x3_walk"
+                               if meta["n"] > 2_000_000 else
+                               "plain,batched_bf16,batched_bf16x3,batched_fp32,batched_bf16x3_walk,host_plain,"
+                               "host_batched_bf16,host_batched_bf16_cached")
     gh = None
     if any(f.startswith("host_") for f in forms_arg.split(",")):
         # records in pinned host memory (use_gpu_mem = false), read over PCIe/C2C
@@ -793,6 +809,9 @@ def _run_ours(args, rank, world, local):
                 f"{'SIFT' if meta['kind'] == 'u8' else 'DEEP'}; index built on the device",
         "config": config_of(meta, nq, k),
         "form": head, "L": r["L"], "parallelism": f"replicas x{world}",
+        "entry": ("the pivot-graph walk (plain form: the reference's)" if head == "plain" or
+                  getattr(runner, "entry", 0) == 0 else
+                  "nearest pivot of the pivot file, one tensor-core product per batch (gann_nearest_pivots)"),
         "beam_width": (tuned["beam_width"] if tuned else args.beam) if head != "plain" else 1, "autotune": tuned,
         "l2_flush": "256 MB write before every GPU step, outside the timed span",
         "recall": r["recall"], "recall_unique": r["recall_unique"], "recall_target": args.recall,
@@ -954,6 +973,8 @@ def main():
                     help="HBM record cache of the host_batched_bf16_cached form, as a fraction of the page bytes")
     ap.add_argument("--headline", default="batched_bf16x3")
     ap.add_argument("--beam", type=int, default=0, help="0 = autotune (gann_autotune)")
+    ap.add_argument("--entry", choices=["nearest", "walk"], default="nearest",
+                    help="entry of the batched forms: the nearest pivot (tensor cores) or the pivot-graph walk")
     ap.add_argument("--tune-L", type=int, default=384)
     ap.add_argument("--batch", type=int, default=0, help="queries per step (default: all --nq)")
     ap.add_argument("--no-precision", dest="precision", action="store_false",
@@ -966,6 +987,8 @@ def main():
     ap.add_argument("--serve-batch", type=int, default=1024)
     ap.add_argument("--serve-streams", type=int, default=8)
     args = ap.parse_args()
+    global ENTRY
+    ENTRY = 1 if args.entry == "nearest" else 0
     rank, world, local = dist_env()
     if args.prepare_only:
         build_workload(args.workload, args.nq, Path(args.cache))

@@ -27,6 +27,7 @@ _lib = None
 GANN_OK, GANN_EINVAL, GANN_EIO, GANN_EFORMAT, GANN_ECUDA, GANN_ENOMEM, GANN_EKERNEL, GANN_ERANGE, GANN_EBUSY = range(9)
 GANN_OPEN_NO_VALIDATE, GANN_OPEN_HOST_PAGES = 1, 2
 PREC_FP32, PREC_BF16, PREC_BF16X3, PREC_BF16_CC = 0, 1, 2, 3
+ENTRY_NAV_WALK, ENTRY_NEAREST_PIVOT = 0, 1
 
 
 class DataType(enum.IntEnum):
@@ -62,7 +63,7 @@ class BatchOpts(ctypes.Structure):
     """gann_batch_opts_t (include/gann.h)."""
 
     _fields_ = [("precision", ctypes.c_int32), ("beam_width", ctypes.c_int32), ("hash_bits", ctypes.c_int32),
-                ("reserved", ctypes.c_int32 * 5)]
+                ("entry", ctypes.c_int32), ("reserved", ctypes.c_int32 * 4)]
 
 
 class ServerOpts(ctypes.Structure):
@@ -71,7 +72,7 @@ class ServerOpts(ctypes.Structure):
     _fields_ = [("max_batch", ctypes.c_int32), ("streams", ctypes.c_int32), ("topk_max", ctypes.c_int32),
                 ("ef_max", ctypes.c_int32), ("precision", ctypes.c_int32), ("beam_width", ctypes.c_int32),
                 ("hash_bits", ctypes.c_int32), ("max_wait_us", ctypes.c_int32), ("min_batch", ctypes.c_int32),
-                ("mem_budget_kib", ctypes.c_int32), ("reserved", ctypes.c_int32 * 6)]
+                ("mem_budget_kib", ctypes.c_int32), ("entry", ctypes.c_int32), ("reserved", ctypes.c_int32 * 5)]
 
 
 class LoadStats(ctypes.Structure):
@@ -114,6 +115,7 @@ _SIGNATURES = {
     "gann_server_start": (_I, [_P, ctypes.POINTER(ServerOpts), ctypes.POINTER(_P)]),
     "gann_server_submit": (_I, [_P, _P, _I, _I, ctypes.c_uint64]),
     "gann_server_request_bytes": (ctypes.c_int64, [_P, _I, _I]),
+    "gann_nearest_pivots": (_I, [_P, _P, _I, _P, _P, _P]),
     "gann_server_poll": (_I, [_P, _I, _P, _P, _P, _P, _P, ctypes.POINTER(_I)]),
     "gann_server_stop": (_I, [_P]),
     "gann_server_open_loop": (_I, [_P, _P, _I, _P, _P, ctypes.c_double, ctypes.c_double, ctypes.c_uint64,
@@ -253,13 +255,13 @@ class GustANN:
                                            d_hops or None, d_bytes or None, _stream(stream)))
 
     @staticmethod
-    def _opts(precision, beam_width, hash_bits):
+    def _opts(precision, beam_width, hash_bits, entry=ENTRY_NAV_WALK):
         o = BatchOpts()
-        o.precision, o.beam_width, o.hash_bits = int(precision), int(beam_width), int(hash_bits)
+        o.precision, o.beam_width, o.hash_bits, o.entry = int(precision), int(beam_width), int(hash_bits), int(entry)
         return o
 
     def search_batch(self, q: np.ndarray, topk, ef_search, precision: int = PREC_BF16, beam_width: int = 0,
-                     hash_bits: int = 0):
+                     hash_bits: int = 0, entry: int = ENTRY_NAV_WALK):
         """Batched search (gann_search_batch). ``topk`` / ``ef_search`` are ints or
         per-query int arrays. Returns (ids nq x kmax, distances, found, seconds)."""
         q = np.ascontiguousarray(q, dtype=np.float32)
@@ -272,7 +274,7 @@ class GustANN:
         dis = np.zeros((nq, kmax), np.float32)
         fnd = np.zeros(nq, np.int32)
         t = ctypes.c_double(0.0)
-        o = self._opts(precision, beam_width, hash_bits)
+        o = self._opts(precision, beam_width, hash_bits, entry)
         _check(lib().gann_search_batch(self.handle, _ptr(q), nq, None if karr is None else _ptr(karr),
                                        None if larr is None else _ptr(larr), kmax, lmax, ctypes.byref(o),
                                        _ptr(nns), _ptr(dis), _ptr(fnd), ctypes.byref(t)))
@@ -281,11 +283,15 @@ class GustANN:
     def search_batch_device(self, d_q: int, nq: int, d_topk: int, d_ef: int, topk_max: int, ef_max: int,
                             d_nns: int, d_dists: int, d_found: int, d_hops: int = 0, d_bytes: int = 0,
                             precision: int = PREC_BF16, beam_width: int = 0, hash_bits: int = 0,
-                            stream: int | None = None) -> None:
-        o = self._opts(precision, beam_width, hash_bits)
+                            stream: int | None = None, entry: int = ENTRY_NAV_WALK) -> None:
+        o = self._opts(precision, beam_width, hash_bits, entry)
         _check(lib().gann_search_batch_device(self.handle, d_q, nq, d_topk or None, d_ef or None, topk_max, ef_max,
                                               ctypes.byref(o), d_nns, d_dists, d_found, d_hops or None,
                                               d_bytes or None, _stream(stream)))
+
+    def nearest_pivots(self, d_q: int, nq: int, d_pivot: int, d_node: int, stream: int | None = None) -> None:
+        """gann_nearest_pivots: per query, the nearest pivot's row and node id (device buffers)."""
+        _check(lib().gann_nearest_pivots(self.handle, d_q, nq, d_pivot or None, d_node or None, _stream(stream)))
 
     def autotune(self, d_q: int, nq: int, topk: int, ef_search: int, precision: int = PREC_BF16):
         """gann_autotune: returns (beam_width, hash_bits, seconds) of the fastest
@@ -362,13 +368,13 @@ class Server:
 
     def __init__(self, index: GustANN, max_batch: int = 1024, streams: int = 4, topk_max: int = 100,
                  ef_max: int = 512, precision: int = PREC_BF16X3, beam_width: int = 0, hash_bits: int = 0,
-                 max_wait_us: int = 100, min_batch: int = 0, mem_budget_kib: int = 0):
+                 max_wait_us: int = 100, min_batch: int = 0, mem_budget_kib: int = 0, entry: int = ENTRY_NAV_WALK):
         self.index = index
         self.dim = index.info()["dim"]
         o = ServerOpts()
         (o.max_batch, o.streams, o.topk_max, o.ef_max, o.precision, o.beam_width, o.hash_bits, o.max_wait_us,
-         o.min_batch, o.mem_budget_kib) = (max_batch, streams, topk_max, ef_max, precision, beam_width, hash_bits,
-                                           max_wait_us, min_batch, mem_budget_kib)
+         o.min_batch, o.mem_budget_kib, o.entry) = (max_batch, streams, topk_max, ef_max, precision, beam_width,
+                                                    hash_bits, max_wait_us, min_batch, mem_budget_kib, entry)
         self.topk_max = topk_max
         self._s = _P()
         _check(lib().gann_server_start(index.handle, ctypes.byref(o), ctypes.byref(self._s)))

@@ -28,7 +28,7 @@ NVCC_FLAGS = [
 EXPORTS = [
     "gann_open", "gann_close", "gann_get_info", "gann_search", "gann_search_device", "gann_search_device_ex", "gann_search_batch", "gann_search_batch_device", "gann_search_batch_noalloc", "gann_pq_tables", "gann_autotune", "gann_server_start", "gann_server_submit", "gann_server_request_bytes", "gann_server_poll", "gann_server_stop", "gann_server_open_loop", "gann_check",
     "gann_set_fma", "gann_last_error", "gann_sample_pivots", "gann_batch_graph_create",
-    "gann_batch_graph_launch", "gann_batch_graph_destroy", "gann_cache_hot_records", "gann_build_prune",
+    "gann_batch_graph_launch", "gann_batch_graph_destroy", "gann_cache_hot_records", "gann_build_prune", "gann_nearest_pivots",
 ]
 
 

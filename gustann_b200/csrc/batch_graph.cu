@@ -1,7 +1,8 @@
 // Batched search captured once as a CUDA graph and replayed.
 //
 // The graph holds the whole batch: the work-counter reset, the tensor-core
-// table build and the persistent walk, whose CTAs pull query indices from the
+// table build, the nearest-pivot entry search when the options ask for it,
+// and the persistent walk, whose CTAs pull query indices from the
 // counter. Buffers are fixed at capture; the number of queries of a launch is
 // read by the kernels from device memory, so one graph serves every batch size
 // up to its maximum and a producer on the device or the host only has to write
@@ -15,7 +16,7 @@ int gann_internal_set_error(int code, const char* msg);
 int gann_internal_enqueue_batch_dev(gann_t* h, const float* d_q, int nq, const int32_t* d_k, const int32_t* d_l,
                                     int k_max, int l_max, const gann_batch_opts_t* opts, int32_t* d_nns,
                                     float* d_dists, int32_t* d_found, cudaStream_t s, int* counter,
-                                    __nv_bfloat16* tables, const int* nq_dev);
+                                    __nv_bfloat16* tables, const int* nq_dev, unsigned long long* entry_keys);
 
 struct gann_batch_graph {
   int device = 0;
@@ -24,6 +25,7 @@ struct gann_batch_graph {
   cudaGraphExec_t exec = nullptr;
   int* counter = nullptr;
   __nv_bfloat16* tables = nullptr;
+  unsigned long long* entry_keys = nullptr;  // nearest-pivot keys (GANN_ENTRY_NEAREST_PIVOT)
 };
 
 namespace {
@@ -33,6 +35,7 @@ void release(gann_batch_graph* g) {
   if (g->graph) cudaGraphDestroy(g->graph);
   if (g->counter) cudaFree(g->counter);
   if (g->tables) cudaFree(g->tables);
+  if (g->entry_keys) cudaFree(g->entry_keys);
   if (g->stream) cudaStreamDestroy(g->stream);
   delete g;
 }
@@ -69,6 +72,8 @@ int gann_batch_graph_create(gann_t* h, int max_nq, int topk_max, int ef_max, con
   if (e == cudaSuccess) e = cudaMalloc(&g->counter, sizeof(int));
   if (e == cudaSuccess && (prec == GANN_PREC_BF16 || prec == GANN_PREC_BF16X3))
     e = cudaMalloc(&g->tables, sizeof(__nv_bfloat16) * (size_t)max_nq * h->hx.pq_m * gann::kPivots);
+  if (e == cudaSuccess && opts && opts->entry == GANN_ENTRY_NEAREST_PIVOT)
+    e = cudaMalloc(&g->entry_keys, sizeof(unsigned long long) * (size_t)max_nq);
   if (e != cudaSuccess) {
     rc = cuda_error("batch graph buffers", e);
   } else {
@@ -79,7 +84,7 @@ int gann_batch_graph_create(gann_t* h, int max_nq, int topk_max, int ef_max, con
     } else {
       rc = gann_internal_enqueue_batch_dev(h, d_queries, max_nq, d_topk, d_ef_search, topk_max, ef_max, opts,
                                            d_nns, d_distances, d_found_cnt, g->stream, g->counter, g->tables,
-                                           d_nq);
+                                           d_nq, g->entry_keys);
       const cudaError_t ee = cudaStreamEndCapture(g->stream, &g->graph);
       if (rc == GANN_OK && ee != cudaSuccess) rc = cuda_error("stream capture", ee);
     }

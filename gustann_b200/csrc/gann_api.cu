@@ -135,10 +135,11 @@ void free_all(gann_index* h) {
   for (void* p : h->allocations) cudaFree(p);
   h->allocations.clear();
   for (void* p : {(void*)h->d_q, (void*)h->d_nns, (void*)h->d_dists, (void*)h->d_found, (void*)h->d_kq,
-                  (void*)h->d_lq, (void*)h->d_tables})
+                  (void*)h->d_lq, (void*)h->d_tables, (void*)h->d_entry})
     if (p) cudaFree(p);
   h->d_kq = h->d_lq = nullptr;
   h->d_tables = nullptr;
+  h->d_entry = nullptr;
   h->d_q = nullptr;
   h->d_nns = nullptr;
   h->d_dists = nullptr;
@@ -286,6 +287,18 @@ int gann_open(const char* index_file, const char* pq_prefix, const char* nav_dir
         h->dx.tc_groups = tg;
       }
     }
+    if (hx.has_nav) {  // operands of the nearest-pivot entry (entry_tc.cu), when they fit shared memory
+      std::vector<uint8_t> panel;
+      std::vector<float> pn;
+      int nk = 0, tiles = 0;
+      if (gann::entry_tc_smem((int)((hx.dim + 15) / 16)) <= 227 * 1024) {
+        gann::make_entry_panels(hx.nav_data, hx.nav_n, (int)hx.dim, hx.elt, panel, pn, nk, tiles);
+        h->dx.entry_panel = upload(h.get(), panel);
+        h->dx.entry_pnorm = upload(h.get(), pn);
+        h->dx.entry_nk = nk;
+        h->dx.entry_tiles = tiles;
+      }
+    }
     h->d_counter = dev_alloc<int>(h.get(), 1);
     h->d_err = dev_alloc<unsigned int>(h.get(), 1);
     h->dx.err = h->d_err;
@@ -424,13 +437,15 @@ int gann_search(gann_t* h, const float* queries, int nq, int topk, int ef_search
 
 namespace {
 
+cudaError_t entry_scratch(gann_t* h, int nq);
+
 // Enqueue one batched search. counter / tables: caller-owned work counter and
 // BF16 table buffer (nq x M x 256) for concurrent launches; null = the handle's.
 int enqueue_batch(gann_t* h, const float* d_q, int nq, const int32_t* d_k, const int32_t* d_l, int k_max,
                   int l_max, const gann_batch_opts_t* opts, int32_t* d_nns, float* d_dists, int32_t* d_found,
                   int32_t* d_hops, int64_t* d_bytes, cudaStream_t s, int* counter = nullptr,
                   __nv_bfloat16* tables = nullptr, const int* nq_dev = nullptr,
-                  int32_t* visit_count = nullptr) {
+                  int32_t* visit_count = nullptr, unsigned long long* entry_keys = nullptr) {
   gann_batch_opts_t o{};
   if (opts) o = *opts;
   const int prec = opts ? o.precision : GANN_PREC_BF16X3;
@@ -438,6 +453,10 @@ int enqueue_batch(gann_t* h, const float* d_q, int nq, const int32_t* d_k, const
   if (!(W == 1 || W == 2 || W == 4 || W == 8 || W == 16))
     return set_error(GANN_EINVAL, "beam_width must be 1, 2, 4, 8 or 16");
   if (prec < GANN_PREC_FP32 || prec > GANN_PREC_BF16_CC) return set_error(GANN_EINVAL, "unknown precision");
+  if (o.entry != GANN_ENTRY_NAV_WALK && o.entry != GANN_ENTRY_NEAREST_PIVOT)
+    return set_error(GANN_EINVAL, "unknown entry");
+  if (o.entry == GANN_ENTRY_NEAREST_PIVOT && !h->dx.entry_panel)
+    return set_error(GANN_ERANGE, "the nearest-pivot entry needs a pivot graph and dim <= 176");
   const int hb = o.hash_bits ? o.hash_bits : gann::batch_hash_bits(l_max) + h->tuned_hash_delta;
   if (hb < 4 || hb > 16) return set_error(GANN_EINVAL, "hash_bits must be in 4..16");
   const bool bf16 = prec != GANN_PREC_FP32;
@@ -496,11 +515,30 @@ int enqueue_batch(gann_t* h, const float* d_q, int nq, const int32_t* d_k, const
     if (e != cudaSuccess) return set_error(GANN_ECUDA, std::string("table build: ") + cudaGetErrorString(e));
     p.tables = tab;
   }
+  if (o.entry == GANN_ENTRY_NEAREST_PIVOT) {
+    if (!entry_keys && entry_scratch(h, nq) != cudaSuccess)
+      return set_error(GANN_ENOMEM, "cannot allocate the batch's entry keys");
+    unsigned long long* keys = entry_keys ? entry_keys : h->d_entry;
+    e = gann::launch_entry_tc(h->dx, (int)h->hx.dim, d_q, nq, keys, s, h->num_sms, nq_dev);
+    if (e != cudaSuccess) return set_error(GANN_ECUDA, std::string("entry search: ") + cudaGetErrorString(e));
+    p.entry_keys = keys;
+  }
   if (d_bytes) e = cudaMemsetAsync(d_bytes, 0, sizeof(int64_t) * nq, s);
   if (e == cudaSuccess) e = cudaMemsetAsync(p.next_query, 0, sizeof(int), s);
   if (e == cudaSuccess) e = gann::launch_batch(p, h->hx.dtype, bf16, W, h->num_sms, s);
   if (e != cudaSuccess) return set_error(GANN_ECUDA, std::string("batch search launch: ") + cudaGetErrorString(e));
   return GANN_OK;
+}
+
+// The handle's entry-key scratch, grown to nq keys.
+cudaError_t entry_scratch(gann_t* h, int nq) {
+  if ((size_t)nq <= h->cap_entry) return cudaSuccess;
+  if (h->d_entry) cudaFree(h->d_entry);
+  h->d_entry = nullptr;
+  h->cap_entry = 0;
+  const cudaError_t e = cudaMalloc(&h->d_entry, sizeof(unsigned long long) * (size_t)nq);
+  if (e == cudaSuccess) h->cap_entry = (size_t)nq;
+  return e;
 }
 
 int check_batch_args(const gann_t* h, int nq, int k_max, int l_max) {
@@ -527,6 +565,22 @@ int gann_search_batch_device(gann_t* h, const float* d_queries, int nq, const in
   cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
   return enqueue_batch(h, d_queries, nq, d_topk, d_ef_search, topk_max, ef_max, opts, d_nns, d_distances,
                        d_found_cnt, d_hops, d_bytes, s);
+}
+
+int gann_nearest_pivots(gann_t* h, const float* d_queries, int nq, int32_t* d_pivot, int32_t* d_node,
+                        void* stream) {
+  if (!h) return set_error(GANN_EINVAL, "null handle");
+  if (nq < 0) return set_error(GANN_EINVAL, "nq must be >= 0");
+  if (nq == 0) return GANN_OK;
+  if (!d_queries) return set_error(GANN_EINVAL, "null buffer");
+  if (!h->dx.entry_panel) return set_error(GANN_ERANGE, "the nearest-pivot entry needs a pivot graph and dim <= 176");
+  std::lock_guard<std::mutex> lk(h->mu);
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
+  if (entry_scratch(h, nq) != cudaSuccess) return set_error(GANN_ENOMEM, "cannot allocate the entry keys");
+  cudaError_t e = gann::launch_entry_tc(h->dx, (int)h->hx.dim, d_queries, nq, h->d_entry, s, h->num_sms);
+  if (e == cudaSuccess) e = gann::launch_entry_ids(h->dx, h->hx.nav_n, h->d_entry, nq, d_pivot, d_node, s);
+  if (e != cudaSuccess) return set_error(GANN_ECUDA, std::string("nearest pivots: ") + cudaGetErrorString(e));
+  return GANN_OK;
 }
 
 int gann_search_batch(gann_t* h, const float* queries, int nq, const int32_t* topk, const int32_t* ef_search,
@@ -734,9 +788,9 @@ int gann_set_fma(gann_t* h, int fma_table, int fma_exact) {
 int gann_internal_enqueue_batch_dev(gann_t* h, const float* d_q, int nq, const int32_t* d_k, const int32_t* d_l,
                                     int k_max, int l_max, const gann_batch_opts_t* opts, int32_t* d_nns,
                                     float* d_dists, int32_t* d_found, cudaStream_t s, int* counter,
-                                    __nv_bfloat16* tables, const int* nq_dev) {
+                                    __nv_bfloat16* tables, const int* nq_dev, unsigned long long* entry_keys) {
   return enqueue_batch(h, d_q, nq, d_k, d_l, k_max, l_max, opts, d_nns, d_dists, d_found, nullptr, nullptr, s,
-                       counter, tables, nq_dev);
+                       counter, tables, nq_dev, nullptr, entry_keys);
 }
 
 extern "C" int gann_cache_hot_records(gann_t* h, const float* d_queries, int nq, int ef_search, int64_t max_bytes,

@@ -90,6 +90,10 @@ struct DeviceIndex {
   const uint8_t* tc_bpanel_lo = nullptr;  // M x 8 KB
   const float* tc_pnorm = nullptr;        // M x 256
   int tc_p = 0, tc_groups = 0;            // padded chunk width, chunk groups per K=16 slice
+  // nearest-pivot entry (entry_tc.cu): pivot tiles of 256 x nk K=16 slices, squared norms
+  const uint8_t* entry_panel = nullptr;   // entry_tiles x entry_nk x 8 KB
+  const float* entry_pnorm = nullptr;     // entry_tiles x 256
+  int entry_nk = 0, entry_tiles = 0;
   unsigned int* err = nullptr;            // kernel error word
   // HBM copies of hot records when the pages sit in host memory
   // (gann_cache_hot_records): rec_remap[u] = cache slot of node u, or -1.
@@ -144,6 +148,7 @@ struct BatchParams {
   FastDiv npp_div;                // division by nodes per page
   int32_t* visit_count;           // or null: per-node expansion counts (gann_cache_hot_records)
   const __nv_bfloat16* tables;    // nq x M x 256 BF16 tables built for the batch, or null
+  const unsigned long long* entry_keys;  // nq: nearest-pivot keys (entry_tc.cu), or null (pivot-graph walk)
   int fma;
   int32_t* nns;                   // nq x k_max
   float* dists;                   // nq x k_max
@@ -181,6 +186,18 @@ size_t table_tc_smem(int M, int groups);
 // tables[q][c][j] = |r_qc|^2 - 2 r_qc . P_cj + |P_cj|^2 with r = q - centroid.
 cudaError_t launch_table_tc(const DeviceIndex& ix, int dim, int M, const float* queries, int nq, int split3,
                             __nv_bfloat16* tables, cudaStream_t stream, int num_sms, const int* nq_dev = nullptr);
+
+// Nearest pivot of every query on the tensor cores (entry_tc.cu): keys[q] =
+// (ordered bits of |x|^2 - 2 q.x) << 32 | pivot index, the minimum over the
+// pivot file; all bits set when the file is empty.
+void make_entry_panels(const std::vector<uint8_t>& data, int nav_n, int dim, int elt, std::vector<uint8_t>& panel,
+                       std::vector<float>& pnorm, int& nk_out, int& ntiles_out);
+size_t entry_tc_smem(int nk);
+cudaError_t launch_entry_tc(const DeviceIndex& ix, int dim, const float* queries, int nq, unsigned long long* keys,
+                            cudaStream_t stream, int num_sms, const int* nq_dev = nullptr);
+// Pivot row (or -1) and node id (or -1) of each key; either output may be null.
+cudaError_t launch_entry_ids(const DeviceIndex& ix, int nav_n, const unsigned long long* keys, int nq, int32_t* pivot,
+                             int32_t* node, cudaStream_t stream);
 
 // Per-warp shared-memory footprint of the plain kernel, in bytes.
 size_t plain_smem_per_warp(int M, int L, int max_m, int k, int dim);
@@ -225,6 +242,8 @@ struct gann_index {
   size_t cap_kq = 0, cap_lq = 0;
   __nv_bfloat16* d_tables = nullptr; // BF16 tables of one batch (scratch)
   size_t cap_tables = 0;
+  unsigned long long* d_entry = nullptr;  // nearest-pivot keys of one batch (scratch)
+  size_t cap_entry = 0;
   int fma_table = 1, fma_exact = 1;
   int tuned_beam = 0;       // batched-form defaults chosen by gann_autotune (0 = built-in)
   int tuned_hash_delta = 0; // added to the L-sized visited-cache bits

@@ -65,6 +65,8 @@ extern "C" int gann_search_batch_noalloc(gann_t* h, const float* d_queries, int 
   if (!(W == 1 || W == 2 || W == 4 || W == 8 || W == 16))
     return gann_internal_set_error(GANN_EINVAL, "beam_width must be 1, 2, 4, 8 or 16");
   if (prec < GANN_PREC_FP32 || prec > GANN_PREC_BF16_CC) return gann_internal_set_error(GANN_EINVAL, "unknown precision");
+  if (o.entry != GANN_ENTRY_NAV_WALK)
+    return gann_internal_set_error(GANN_EINVAL, "gann_search_batch_noalloc enters by the pivot-graph walk only");
   const bool tc = prec == GANN_PREC_BF16 || prec == GANN_PREC_BF16X3;
   if (tc && nq > kNoAllocMaxQueries)
     return gann_internal_set_error(GANN_ERANGE,

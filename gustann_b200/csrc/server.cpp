@@ -130,11 +130,12 @@ cudaError_t alloc_slot(Slot& s, int B, int dim, int kmax) {
 // candidate list (id + distance per entry), the visited cache (one id per
 // slot, sized from L as the batched form sizes it), the PQ table (BF16 or
 // FP32 per precision), the query and the result row (id + distance per k,
-// plus the found count).
+// plus the found count), and the entry key with the nearest-pivot entry.
 int64_t request_bytes(const gann_server* sv, int k, int L) {
   const int tab = sv->o.precision == GANN_PREC_FP32 ? 4 : 2;
   const int hb = sv->o.hash_bits ? sv->o.hash_bits : gann::batch_hash_bits(L);
-  return 8ll * L + 4ll * (1ll << hb) + (int64_t)tab * sv->M * gann::kPivots + 4ll * sv->dim + 8ll * k + 4;
+  return 8ll * L + 4ll * (1ll << hb) + (int64_t)tab * sv->M * gann::kPivots + 4ll * sv->dim + 8ll * k + 4 +
+         (sv->o.entry == GANN_ENTRY_NEAREST_PIVOT ? 8 : 0);
 }
 
 // Publish a finished batch into the completion ring. Dispatcher thread only.
@@ -329,6 +330,7 @@ int gann_server_start(gann_t* h, const gann_server_opts_t* opts, gann_server_t**
   bo.precision = o.precision;
   bo.beam_width = o.beam_width;
   bo.hash_bits = o.hash_bits;
+  bo.entry = o.entry;
   for (Slot& s : sv->slots) {
     e = alloc_slot(s, o.max_batch, sv->dim, o.topk_max);
     if (e != cudaSuccess) break;

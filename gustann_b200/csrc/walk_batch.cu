@@ -2,7 +2,8 @@
 //
 // One CTA of W warps serves one query at a time and pulls the next query from a
 // device counter (persistent grid). Per query: the pivot-graph entry walk
-// (src/impl/nav.cuh:13-135) on warp 0 while the other warps build the PQ table
+// (src/impl/nav.cuh:13-135) on warp 0, or the nearest pivot found for the
+// whole batch on the tensor cores (entry_tc.cu), while the other warps build the PQ table
 // (src/impl/pq.cuh:8-59) in shared memory, FP32 or BF16 (or copy a BF16 table
 // built on the tensor cores for the whole batch); then a beam walk that expands
 // up to W candidates per step, one per warp (src/impl/pure_mem.cuh:243-432
@@ -346,7 +347,18 @@ __global__ void __launch_bounds__(W * 32, W <= 8 ? 24 / W : 2) batch_search_kern
     __syncthreads();
     int64_t gathered = 0;  // per-warp share of the algorithmic bytes
     if (warp == 0) {
-      int64_t u0 = entry_node<T>(p.has_nav, nv, p.medoid, s.q, lane, gathered);
+      int64_t u0;
+      if (p.entry_keys) {  // the nearest pivot, found for the batch on the tensor cores (entry_tc.cu)
+        const uint32_t local = (uint32_t)__ldg(p.entry_keys + qid);
+        if (local < (uint32_t)p.nav_n) {
+          u0 = __ldg(p.ix.nav_map + local);
+        } else {
+          if (lane == 0) atomicOr(p.err, kErrBadId);
+          u0 = -2;
+        }
+      } else {
+        u0 = entry_node<T>(p.has_nav, nv, p.medoid, s.q, lane, gathered);
+      }
       if (lane == 0) s.ctrl[3] = (int)u0;
     }
     if (p.tables) {  // BF16 tables built for the whole batch on the tensor cores

@@ -57,6 +57,16 @@ enum {
   GANN_PREC_BF16_CC = 3  /* BF16 tables built per query on CUDA cores (FP32 then rounded) */
 };
 
+/* entry node of the batched form's walk */
+enum {
+  GANN_ENTRY_NAV_WALK = 0,      /* the reference's greedy walk over the pivot graph, a beam of 4
+                                   (src/impl/nav.cuh:13-135), or the medoid without a pivot graph */
+  GANN_ENTRY_NEAREST_PIVOT = 1  /* the nearest point of the pivot file (nav_index.data) by squared L2,
+                                   found for the whole batch as one tensor-core product of the queries
+                                   by the pivots (exact for uint8 vectors and integral queries; float
+                                   operands rounded to BF16). Needs a pivot graph and dim <= 176. */
+};
+
 /* options of gann_search_batch; zero-initialised = defaults, except that a
  * zero precision is GANN_PREC_FP32. Passing opts = NULL selects
  * GANN_PREC_BF16X3: the split-BF16 tensor-core tables, whose error against
@@ -66,7 +76,8 @@ typedef struct {
   int32_t precision;   /* GANN_PREC_*; opts = NULL means GANN_PREC_BF16X3 */
   int32_t beam_width;  /* warps (nodes expanded per step) per query: 1, 2, 4, 8 or 16; 0 = 4 (or autotuned) */
   int32_t hash_bits;   /* visited cache of 2^hash_bits ids per query; 0 = sized from L */
-  int32_t reserved[5];
+  int32_t entry;       /* GANN_ENTRY_*; 0 (and opts = NULL) = GANN_ENTRY_NAV_WALK */
+  int32_t reserved[4];
 } gann_batch_opts_t;
 
 typedef struct {
@@ -189,6 +200,19 @@ int gann_search_device_ex(gann_t* h, const float* d_queries, int nq, int topk, i
                           int64_t* d_bytes, void* stream);
 
 /*
+ * The nearest point of the pivot file (nav_index.data) of each query, the
+ * entry node of GANN_ENTRY_NEAREST_PIVOT: d_pivot[q] = its row in the pivot
+ * file, d_node[q] = its node id (map.txt); either output may be NULL. Device
+ * buffers, enqueued on `stream` (NULL = the handle's stream). Exact for uint8
+ * vectors with integral queries (ties to the lowest row); float operands are
+ * rounded to BF16. GANN_ERANGE without a pivot graph or above dim 176. The
+ * reference's entry is the pivot-graph walk (src/impl/nav.cuh:13-135,
+ * src/nav_graph.cu:104-109); this is an exact search over the same points.
+ */
+int gann_nearest_pivots(gann_t* h, const float* d_queries, int nq, int32_t* d_pivot, int32_t* d_node,
+                        void* stream);
+
+/*
  * gann_search_batch_device for callers that cannot allocate device memory
  * while they search: a serving loop that must not stall on cudaMalloc (which
  * can synchronise the device and takes the driver's allocation lock), or a
@@ -200,7 +224,8 @@ int gann_search_device_ex(gann_t* h, const float* d_queries, int nq, int topk, i
  * (work counter, BF16 tables) is a fixed 8 MiB + 256 B array inside the
  * library, held on every GPU that loads libgann until the process exits.
  * Options left 0 (or opts NULL) take the same defaults as
- * gann_search_batch_device, the handle's gann_autotune choices included.
+ * gann_search_batch_device, the handle's gann_autotune choices included; the
+ * entry is the pivot-graph walk (GANN_ENTRY_NEAREST_PIVOT returns GANN_EINVAL).
  * Limits, tensor-core tables (GANN_PREC_BF16, GANN_PREC_BF16X3) only: nq <= 512
  * per call and at most 32 PQ chunks; larger requests return GANN_ERANGE. The
  * FP32 and CUDA-core BF16 precisions use only the work counter and take any nq.
@@ -275,7 +300,8 @@ typedef struct {
   int32_t max_wait_us;  /* a batch smaller than min_batch waits this long for company; 0 = 100 */
   int32_t min_batch;    /* 0 = launch as soon as a slot is free */
   int32_t mem_budget_kib; /* admission budget in KiB; 0 = every request slot at (topk_max, ef_max) */
-  int32_t reserved[6];
+  int32_t entry;        /* GANN_ENTRY_* of every batch; 0 = the pivot-graph walk */
+  int32_t reserved[5];
 } gann_server_opts_t;
 
 typedef struct {

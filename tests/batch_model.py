@@ -58,9 +58,11 @@ class BatchModel:
             return np.float32(int(((q.astype(np.int64) - v.astype(np.int64)) ** 2).sum()))
         return np.float32(self.om.exact_dist(q, v, True))
 
-    def search(self, queries, k, L, W):
+    def search(self, queries, k, L, W, entries=None):
+        """entries: the entry node of each query, or None for the pivot-graph
+        walk's (the oracle's nav walk)."""
         queries = np.ascontiguousarray(queries, dtype=np.float32)
-        ents = self.o.search(queries, 1, 1)[5]
+        ents = self.o.search(queries, 1, 1)[5] if entries is None else np.asarray(entries)
         nq = len(queries)
         ids = np.zeros((nq, k), np.int32)
         dis = np.zeros((nq, k), np.float32)

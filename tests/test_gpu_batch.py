@@ -264,3 +264,159 @@ def test_batched_fp32_matches_cpu_model(golden, oracle_mod, name):
         assert bad.size == 0, f"{what}: {bad.size} queries differ, first {bad[:5]}"
         np.testing.assert_array_equal(dis.view(np.uint32), md.view(np.uint32), err_msg=what)
     g.check()
+
+
+def read_pivots(meta):
+    """(pivot vectors nav_n x dim, node id of each) from the fixture's pivot graph."""
+    import struct
+
+    d = Path(meta["nav_dir"])
+    raw = (d / "nav_index.data").read_bytes()
+    n, dim = struct.unpack_from("<ii", raw, 0)
+    data = np.frombuffer(raw, np.uint8 if meta["dtype"] == 0 else np.float32, count=n * dim, offset=8)
+    return data.reshape(n, dim), np.loadtxt(d / "map.txt", dtype=np.int64).reshape(-1)
+
+
+def nearest_pivots(g, q):
+    import torch
+
+    dq = torch.from_numpy(np.ascontiguousarray(q, dtype=np.float32)).cuda()
+    piv = torch.full((len(q),), -7, dtype=torch.int32, device="cuda")
+    node = torch.full((len(q),), -7, dtype=torch.int32, device="cuda")
+    g.nearest_pivots(dq.data_ptr(), len(q), piv.data_ptr(), node.data_ptr())
+    torch.cuda.synchronize()
+    g.check()
+    return piv.cpu().numpy(), node.cpu().numpy()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["u8_nav", "f32_nav"])
+def test_nearest_pivot_entry_is_the_nearest_pivot(golden, name):
+    """gann_nearest_pivots (the tensor-core product of queries by pivots with an
+    argmin epilogue) against brute force in FP64: for uint8 vectors and
+    integral queries the same row, ties to the lowest; for float vectors a
+    pivot within the BF16 rounding of the operands. Batches of 1, 100 and all
+    queries (one and several CTAs per pivot range)."""
+    meta = golden[name]
+    g = open_meta(meta)
+    data, node_of = read_pivots(meta)
+    q = meta["queries"]
+    d = ((q.astype(np.float64)[:, None, :] - data.astype(np.float64)[None, :, :]) ** 2).sum(-1)
+    best = d.argmin(1)  # first index of the minimum
+    for nq in (1, 100, len(q)):
+        piv, node = nearest_pivots(g, q[:nq])
+        assert (piv >= 0).all() and (piv < len(data)).all()
+        np.testing.assert_array_equal(node, node_of[piv])
+        rows = np.arange(nq)
+        if meta["dtype"] == 0:
+            np.testing.assert_array_equal(piv, best[:nq])
+        else:
+            # BF16 operands: each product q_i x_i is off by at most 2^-8 |q_i x_i|
+            # (both roundings), each |x|^2 term by 2^-8 |x|^2
+            qx = np.abs(q[:nq].astype(np.float64)) @ np.abs(data.astype(np.float64)).T
+            tol = 2.0 ** -7 * (2.0 * qx[rows, piv] + 2.0 * qx[rows, best[:nq]]) + 2.0 ** -7 * (
+                (data.astype(np.float64) ** 2).sum(1)[piv] + (data.astype(np.float64) ** 2).sum(1)[best[:nq]])
+            assert (d[rows, piv] - d[rows, best[:nq]] <= tol).all()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["u8_nav", "f32_nav"])
+def test_nearest_pivot_entry_walk_matches_cpu_model(golden, oracle_mod, name):
+    """With GANN_ENTRY_NEAREST_PIVOT and FP32 tables the batched form equals the
+    cache-free CPU model started from the same entry nodes, bit for bit; the
+    recall at L 40 is at least the pivot-graph walk's minus 0.02."""
+    from batch_model import BatchModel
+
+    meta = golden[name]
+    model = BatchModel(oracle_mod, meta)
+    g = open_meta(meta)
+    q = meta["queries"][:100]
+    _, node = nearest_pivots(g, q)
+    for k, L, W, hb in ((10, 40, 4, 4), (10, 64, 8, 5), (5, 32, 16, 4)):
+        ids, dis, fnd, _ = g.search_batch(q, k, L, precision=gb.PREC_FP32, beam_width=W, hash_bits=hb,
+                                          entry=gb.ENTRY_NEAREST_PIVOT)
+        mi, md, mf = model.search(q, k, L, W, entries=node)
+        what = f"{name} k={k} L={L} W={W} hash_bits={hb}"
+        np.testing.assert_array_equal(fnd, mf, err_msg=what)
+        bad = np.nonzero((ids != mi).any(1))[0]
+        assert bad.size == 0, f"{what}: {bad.size} queries differ, first {bad[:5]}"
+        np.testing.assert_array_equal(dis.view(np.uint32), md.view(np.uint32), err_msg=what)
+    qa = meta["queries"]
+    import torch
+
+    from gustann_b200.indexing import formats
+
+    di = formats.read_disk_index(meta["index_file"], np.uint8 if meta["dtype"] == 0 else np.float32)
+
+    gt = groundtruth.knn(torch.from_numpy(np.ascontiguousarray(di.data)), torch.from_numpy(qa), 10)
+    rec = {}
+    for entry in (gb.ENTRY_NAV_WALK, gb.ENTRY_NEAREST_PIVOT):
+        ids, *_ = g.search_batch(qa, 10, 40, precision=gb.PREC_BF16X3, entry=entry)
+        rec[entry] = groundtruth.recall(ids, gt, 10)
+    assert rec[gb.ENTRY_NEAREST_PIVOT] >= rec[gb.ENTRY_NAV_WALK] - 0.02, rec
+    g.check()
+
+
+@pytest.mark.gpu
+def test_nearest_pivot_entry_in_graphs_and_server(golden):
+    """The captured graph and the server take the entry option: a graph replay
+    equals the direct call, the server's results equal the direct call's, and
+    the server charges the entry key in its admission bytes; the no-alloc form
+    and an index without a pivot graph refuse the option."""
+    import torch
+
+    meta = golden["u8_nav"]
+    g = open_meta(meta)
+    q = np.ascontiguousarray(meta["queries"][:64], dtype=np.float32)
+    k, L = 10, 48
+    ids0, dis0, fnd0, _ = g.search_batch(q, k, L, precision=gb.PREC_BF16X3, beam_width=4,
+                                         entry=gb.ENTRY_NEAREST_PIVOT)
+    dq = torch.from_numpy(q).cuda()
+    nq_dev = torch.tensor([len(q)], dtype=torch.int32, device="cuda")
+    ids = torch.zeros((len(q), k), dtype=torch.int32, device="cuda")
+    dis = torch.zeros((len(q), k), dtype=torch.float32, device="cuda")
+    fnd = torch.zeros(len(q), dtype=torch.int32, device="cuda")
+    o = gb.GustANN._opts(gb.PREC_BF16X3, 4, 0, gb.ENTRY_NEAREST_PIVOT)
+    import ctypes
+
+    gr = ctypes.c_void_p()
+    gb._check(gb.lib().gann_batch_graph_create(g.handle, len(q), k, L, ctypes.byref(o), dq.data_ptr(), None, None,
+                                               nq_dev.data_ptr(), ids.data_ptr(), dis.data_ptr(), fnd.data_ptr(),
+                                               ctypes.byref(gr)))
+    try:
+        gb._check(gb.lib().gann_batch_graph_launch(gr, None))
+        torch.cuda.synchronize()
+    finally:
+        gb.lib().gann_batch_graph_destroy(gr)
+    np.testing.assert_array_equal(ids.cpu().numpy(), ids0)
+    np.testing.assert_array_equal(dis.cpu().numpy().view(np.uint32), dis0.view(np.uint32))
+    srv_walk = gb.Server(g, max_batch=32, streams=2, topk_max=k, ef_max=L, precision=gb.PREC_BF16X3,
+                         beam_width=4)
+    srv = gb.Server(g, max_batch=32, streams=2, topk_max=k, ef_max=L, precision=gb.PREC_BF16X3, beam_width=4,
+                    entry=gb.ENTRY_NEAREST_PIVOT)
+    try:
+        assert srv.request_bytes(k, L) == srv_walk.request_bytes(k, L) + 8
+        got = {}
+        for i in range(len(q)):
+            assert srv.submit(q[i], k, L, i)
+        import time
+
+        t0 = time.time()
+        while len(got) < len(q) and time.time() - t0 < 60:
+            tags, ids_r, dis_r, fnd_r, _ = srv.poll(64)
+            for j, tag in enumerate(tags):
+                got[int(tag)] = (ids_r[j], dis_r[j], fnd_r[j])
+        assert len(got) == len(q)
+        for i in range(len(q)):
+            np.testing.assert_array_equal(got[i][0][:fnd0[i]], ids0[i, :fnd0[i]])
+    finally:
+        srv.stop()
+        srv_walk.stop()
+    o2 = gb.GustANN._opts(gb.PREC_BF16X3, 4, 0, gb.ENTRY_NEAREST_PIVOT)
+    rc = gb.lib().gann_search_batch_noalloc(g.handle, dq.data_ptr(), len(q), k, L, ctypes.byref(o2), ids.data_ptr(),
+                                            dis.data_ptr(), fnd.data_ptr(), None)
+    assert rc == gb.GANN_EINVAL
+    gm = open_meta(golden["u8_medoid"])
+    with pytest.raises(gb.GustANNError):
+        gm.search_batch(q, k, L, precision=gb.PREC_BF16X3, entry=gb.ENTRY_NEAREST_PIVOT)
+    g.check()
