@@ -781,8 +781,14 @@ def _run_ours(args, rank, world, local):
     res = {}
     for f in forms:  # a host-paged form runs at the L of its HBM twin (same results, same recall)
         if tuned is None and args.beam == 0 and f != "plain":
-            # autotuner (beam width, visited cache) at the L the plain form needs for the target
-            tune_L = res["plain"]["L"] if "plain" in res else args.tune_L
+            # autotuner (beam width, visited cache) at the L the plain form needs for the target;
+            # when the plain form misses it, at the L this form needs with the built-in defaults
+            if "plain" in res and res["plain"]["recall"] >= args.recall:
+                tune_L = res["plain"]["L"]
+            elif "plain" in res and not f.startswith("host_"):
+                tune_L = calibrate(runners[f], gt, k, args.recall, args.L or None)[0]
+            else:
+                tune_L = res["plain"]["L"] if "plain" in res else args.tune_L
             W, hb, secs = g.autotune(q.data_ptr(), min(q.shape[0], 2000), k, tune_L, gb.PREC_BF16X3)
             tuned = {"beam_width": W, "hash_bits": hb, "at_L": tune_L, "seconds": secs, "queries": min(q.shape[0], 2000)}
         twin = res.get(f[5:].replace("_cached", "")) if f.startswith("host_") else None
