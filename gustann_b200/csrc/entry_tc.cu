@@ -19,6 +19,10 @@
 // into stage i & 1 by one bulk copy, its K slices are multiplied into TMEM
 // columns [256 (i & 1), + 256) and committed to an mbarrier, and while the
 // epilogue drains tile i the MMAs of tile i + 1 run and tile i + 2 is copied.
+// The tile's 256 squared norms are loaded by the CTA's threads (two each)
+// before they wait for the tile's MMAs and stored to norm slot i & 1, which
+// the barrier after that wait publishes; the slot's previous reader (tile
+// i - 2) finished before the barrier that ends iteration i - 2.
 // The CTA's best (value, pivot) of each row is merged into a 64-bit key per
 // query with atomicMin (order-preserving float bits, then the pivot index), so
 // ties go to the lowest pivot index whatever the split.
@@ -62,11 +66,13 @@ __device__ __forceinline__ uint32_t ordered_bits(float f) {
 
 __global__ void __launch_bounds__(kTile, 1) entry_tc_kernel(EntryParams p) {
   extern __shared__ __align__(1024) uint8_t smem[];
-  // [A: nk x 4 KB][B: 2 stages x nk x 8 KB][bars][tmem slot]
+  // [A: nk x 4 KB][B: 2 stages x nk x 8 KB][norms: 2 slots x 1 KB][bars][tmem slot]
   const uint32_t tile_bytes = (uint32_t)p.nk * kBTileBytes;
+  constexpr uint32_t kNormBytes = kN * 4;
   uint8_t* a = smem;
   uint8_t* b = a + (size_t)p.nk * kATileBytes;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(b + 2 * (size_t)tile_bytes);  // [0,1] copies, [2,3] MMAs done
+  uint8_t* norms = b + 2 * (size_t)tile_bytes;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(norms + 2 * kNormBytes);  // [0,1] copies, [2,3] MMAs done
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 4);
   const int tid = threadIdx.x, warp = tid >> 5;
   const int q0 = blockIdx.x * kTile;
@@ -111,8 +117,7 @@ __global__ void __launch_bounds__(kTile, 1) entry_tc_kernel(EntryParams p) {
   auto issue_copy = [&](int i) {
     const int st = i & 1;
     mbar_expect_tx(&bars[st], tile_bytes);
-    bulk_copy_g2s(b + (size_t)st * tile_bytes, p.panel + (size_t)(t_begin + i) * tile_bytes, tile_bytes,
-                  &bars[st]);
+    bulk_copy_g2s(b + (size_t)st * tile_bytes, p.panel + (size_t)(t_begin + i) * tile_bytes, tile_bytes, &bars[st]);
   };
   // tid 0 only: wait for tile i's B slices, then issue its MMAs
   auto issue_mma = [&](int i) -> bool {
@@ -141,26 +146,37 @@ __global__ void __launch_bounds__(kTile, 1) entry_tc_kernel(EntryParams p) {
   for (int i = 0; i < nt && ok; i++) {
     const int st = i & 1;
     bool mine = true;
+    const float* pn = p.pnorm + (size_t)(t_begin + i) * kN;
+    const float n0 = __ldg(pn + tid), n1 = __ldg(pn + kTile + tid);  // in flight during the waits below
     if (tid == 0 && i + 1 < nt) mine = issue_mma(i + 1);  // runs while this tile drains
     mine = mine && mbar_wait(&bars[2 + st], (uint32_t)(i >> 1) & 1u);
+    float* ns = reinterpret_cast<float*>(norms + (size_t)st * kNormBytes);
+    ns[tid] = n0;
+    ns[kTile + tid] = n1;
     ok = __syncthreads_and(mine);
     if (!ok) break;
     tc_fence_after();
     if (tid == 0 && i + 2 < nt) issue_copy(i + 2);  // this stage's B slices are free: MMA i is done
     // Epilogue: row tid of D (TMEM lane tid), |x_j|^2 - 2 q.x_j over the tile's 256 pivots
-    const float* pn = p.pnorm + (size_t)(t_begin + i) * kN;
+    const float4* pn4 = reinterpret_cast<const float4*>(norms + (size_t)st * kNormBytes);
     const uint32_t j0 = (uint32_t)(t_begin + i) * kN;
     const uint32_t dcol = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(st * kN);
-    for (int col = 0; col < kN; col += 16) {
-      uint32_t r[16];
-      tmem_ld16(dcol + (uint32_t)col, r);
+    for (int col = 0; col < kN; col += 32) {
+      uint32_t r[32];
+      tmem_ld32(dcol + (uint32_t)col, r);
       tmem_wait_ld();
 #pragma unroll
-      for (int j = 0; j < 16; j++) {
-        const float v = __fmaf_rn(-2.0f, __uint_as_float(r[j]), __ldg(pn + col + j));
-        if (v < best) {  // strict: the first (lowest) pivot of equal values stays
-          best = v;
-          best_j = j0 + (uint32_t)(col + j);
+      for (int j4 = 0; j4 < 8; j4++) {
+        const float4 n4 = pn4[(col >> 2) + j4];  // the same address in every thread: a broadcast
+        const float nj[4] = {n4.x, n4.y, n4.z, n4.w};
+#pragma unroll
+        for (int t = 0; t < 4; t++) {
+          const int j = 4 * j4 + t;
+          const float v = __fmaf_rn(-2.0f, __uint_as_float(r[j]), nj[t]);
+          if (v < best) {  // strict: the first (lowest) pivot of equal values stays
+            best = v;
+            best_j = j0 + (uint32_t)(col + j);
+          }
         }
       }
     }
@@ -205,7 +221,7 @@ cudaError_t launch_entry_ids(const DeviceIndex& ix, int nav_n, const unsigned lo
   return cudaGetLastError();
 }
 
-size_t entry_tc_smem(int nk) { return (size_t)nk * (kATileBytes + 2 * kBTileBytes) + 32 + 16; }
+size_t entry_tc_smem(int nk) { return (size_t)nk * (kATileBytes + 2 * kBTileBytes) + 2 * kN * 4 + 32 + 16; }
 
 // Host layout of the pivot tiles and their squared norms. data: nav_n x dim
 // elements of elt bytes (uint8 or float32). Pivots past nav_n are zero with an

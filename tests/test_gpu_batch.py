@@ -420,3 +420,38 @@ def test_nearest_pivot_entry_in_graphs_and_server(golden):
     with pytest.raises(gb.GustANNError):
         gm.search_batch(q, k, L, precision=gb.PREC_BF16X3, entry=gb.ENTRY_NEAREST_PIVOT)
     g.check()
+
+
+@pytest.mark.gpu
+def test_nearest_pivots_many_tiles_per_cta(golden, tmp_path):
+    """A pivot file of all 4,000 base points (16 tiles of 256 pivots) and
+    enough queries (149 CTA rows of 128, more than the 148 SMs) that each CTA
+    walks every tile, so
+    the B-stage, norm-slot and TMEM reuse of the tile pipeline all run: the rows
+    equal brute force (uint8, exact), twice in a row."""
+    import torch
+
+    from gustann_b200.indexing import formats
+
+    meta = golden["u8_nav"]
+    data = np.ascontiguousarray(formats.read_disk_index(meta["index_file"], np.uint8).data)
+    n = data.shape[0]
+    deg = np.full(n, 8, dtype=np.int64)
+    graph = ((np.arange(n)[:, None] + np.arange(1, 9)[None, :]) % n).astype(np.int32)
+    nav = tmp_path / "nav_all"
+    formats.write_nav(str(nav), data, graph, deg, 0, np.arange(n))
+    g = gb.GustANN(gb.DataType.UINT8)
+    g.init_pure_mem(gb.GustANNConfig(meta["index_file"], meta["pq_prefix"], str(nav)))
+    rng = np.random.default_rng(5)
+    nq = 149 * 128
+    q = np.clip(data[rng.integers(0, n, nq)].astype(np.int64) + rng.integers(-12, 13, (nq, data.shape[1])), 0, 255)
+    xf = data.astype(np.float64)
+    qf = q.astype(np.float64)
+    d = (qf * qf).sum(1)[:, None] - 2.0 * (qf @ xf.T) + (xf * xf).sum(1)[None, :]  # exact: integers < 2^53
+    want = d.argmin(1)
+    for _ in range(2):
+        piv, node = nearest_pivots(g, q.astype(np.float32))
+        bad = np.nonzero(piv != want)[0]
+        assert bad.size == 0, f"{bad.size} of {nq} queries differ, first {bad[:5]}"
+        np.testing.assert_array_equal(node, want)
+    g.check()
