@@ -317,8 +317,13 @@ struct Record {
   }
 };
 
-template <class T, class TabT, int W, bool PK>
-__global__ void __launch_bounds__(W * 32, W <= 8 ? 24 / W : 2) batch_search_kernel(BatchParams p) {
+// CTAs per SM each kernel is compiled for: 24 warps at up to 80 registers per
+// thread (2 CTAs at 64 for W 16), or, with R64, 32 warps at 64 registers, which
+// the launcher takes when that many CTAs' shared memory fits.
+__host__ __device__ constexpr int min_ctas(int W, bool r64) { return r64 ? 32 / W : (W <= 8 ? 24 / W : 2); }
+
+template <class T, class TabT, int W, bool PK, bool R64>
+__global__ void __launch_bounds__(W * 32, min_ctas(W, R64)) batch_search_kernel(BatchParams p) {
   constexpr int NT = W * 32;
   constexpr int TKW = W - 1;  // warp that marks the picks and keeps the top-k
   extern __shared__ __align__(16) uint8_t smem[];
@@ -710,17 +715,31 @@ __global__ void __launch_bounds__(W * 32, W <= 8 ? 24 / W : 2) batch_search_kern
   }
 }
 
+// CTAs of `kern` that fit one SM with `smem` bytes of dynamic shared memory
+// each (after setting its shared-memory limit), or -1 on an error.
+template <class K>
+int ctas_per_sm(K kern, int W, size_t smem) {
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return -1;
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, W * 32, smem) != cudaSuccess) return -1;
+  return per_sm;
+}
+
 template <class T, class TabT, int W, bool PK>
 cudaError_t launch_wp(const BatchParams& p, int num_sms, cudaStream_t stream) {
   const BatchPlan pl(p.M, (int)sizeof(TabT), 1 << p.hash_bits, p.L_max, p.max_m, W, p.k_max, p.dim);
   const size_t smem = pl.total;
   if (smem > 227 * 1024) return cudaErrorInvalidConfiguration;
-  auto kern = batch_search_kernel<T, TabT, W, PK>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  int per_sm = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, W * 32, smem);
-  if (e != cudaSuccess) return e;
+  auto kern = batch_search_kernel<T, TabT, W, PK, false>;
+  if constexpr (W == 4 || W == 8) {
+    // the 64-register build, when shared memory admits all of its CTAs
+    auto k64 = batch_search_kernel<T, TabT, W, PK, true>;
+    const int n64 = ctas_per_sm(k64, W, smem);
+    if (n64 < 0) return cudaGetLastError();
+    if (n64 >= min_ctas(W, true)) kern = k64;
+  }
+  const int per_sm = ctas_per_sm(kern, W, smem);
+  if (per_sm < 0) return cudaGetLastError();
   if (per_sm < 1) return cudaErrorInvalidConfiguration;
   int grid = num_sms * per_sm;
   if (grid > p.nq) grid = p.nq;
