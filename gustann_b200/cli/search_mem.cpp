@@ -3,7 +3,7 @@
 //
 //   search_mem --query Q.{f,b}vecs --index X_disk.index --pq_data X_pq --data_type uint8|float
 //              [--nav_graph DIR] [--ground_truth GT.ivecs] [--topk K] [--ef_search L [L ...]]
-//              [--repeat|-R N] [--use-gpu-mem|-G] [--batched]
+//              [--repeat|-R N] [--use-gpu-mem|-G] [--batched [--entry walk|nearest]]
 //
 // Same flags and meanings as the reference (search_disk.cpp:51-73): the query
 // set is replicated --repeat times (default 20, :167-179); without -G the
@@ -11,7 +11,9 @@
 // recall (:190-213), several L print an L / run time / QPS / recall table
 // (:214-256). Recall@k counts result ids found among the first k ground-truth
 // ids of the first (unreplicated) queries (utils.hpp:105-117). --batched runs
-// the optimised form (gann_search_batch, BF16 tables) instead of the drop-in.
+// the optimised form (gann_search_batch, BF16X3 tables) instead of the drop-in;
+// --entry nearest starts its walks at each query's nearest pivot
+// (GANN_ENTRY_NEAREST_PIVOT) instead of the pivot-graph walk.
 #include <chrono>
 #include <cstdint>
 #include <cstdio>
@@ -71,7 +73,7 @@ void usage(const char* a0) {
   std::fprintf(stderr,
                "usage: %s --query Q --index I --pq_data P --data_type uint8|float [--nav_graph D]\n"
                "          [--ground_truth G] [--topk K] [--ef_search L [L ...]] [--repeat|-R N] [--use-gpu-mem|-G]\n"
-               "          [--batched]\n",
+               "          [--batched [--entry walk|nearest]]\n",
                a0);
 }
 
@@ -83,6 +85,7 @@ int main(int argc, char** argv) {
   int topk = 100, repeat = 20;
   std::vector<int> efs;
   bool gpu_mem = false, batched = false;
+  std::string entry_s;
   for (int i = 1; i < argc; i++) {
     const std::string a = argv[i];
     auto next = [&]() -> std::string {
@@ -100,6 +103,7 @@ int main(int argc, char** argv) {
       else if (a == "--repeat" || a == "-R") repeat = std::stoi(next());
       else if (a == "--use-gpu-mem" || a == "-G") gpu_mem = true;
       else if (a == "--batched") batched = true;
+      else if (a == "--entry") entry_s = next();
       else if (a == "--ef_search") {
         efs.push_back(std::stoi(next()));
         while (i + 1 < argc && argv[i + 1][0] != '-') efs.push_back(std::stoi(argv[++i]));
@@ -120,6 +124,14 @@ int main(int argc, char** argv) {
   }
   if (dtype_s != "uint8" && dtype_s != "float") {
     std::fprintf(stderr, "unrecognized data type %s\n", dtype_s.c_str());
+    return 1;
+  }
+  if (!entry_s.empty() && entry_s != "walk" && entry_s != "nearest") {
+    std::fprintf(stderr, "unrecognized entry %s (walk or nearest)\n", entry_s.c_str());
+    return 1;
+  }
+  if (!entry_s.empty() && !batched) {
+    std::fprintf(stderr, "--entry applies to --batched only (the drop-in form enters by the pivot-graph walk)\n");
     return 1;
   }
   if (efs.empty()) efs.push_back(300);
@@ -164,7 +176,10 @@ int main(int argc, char** argv) {
         return st.run_time;
       }
       double t = 0.0;
-      const int rc = gann_search_batch(a.handle(), q.data(), (int)nq, nullptr, nullptr, topk, ef, nullptr,
+      gann_batch_opts_t o{};
+      o.precision = GANN_PREC_BF16X3;  // the NULL-options default
+      o.entry = entry_s == "nearest" ? GANN_ENTRY_NEAREST_PIVOT : GANN_ENTRY_NAV_WALK;
+      const int rc = gann_search_batch(a.handle(), q.data(), (int)nq, nullptr, nullptr, topk, ef, &o,
                                        reinterpret_cast<int32_t*>(nns.data()), dis.data(),
                                        reinterpret_cast<int32_t*>(found.data()), &t);
       if (rc != GANN_OK) throw std::runtime_error(std::string("gann_search_batch: ") + gann_last_error());

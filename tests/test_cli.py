@@ -44,6 +44,10 @@ def test_cli_argument_errors(tmp_path):
     assert r.returncode == 1 and "whole number of vectors" in r.stderr
     r = run(["--bogus"])
     assert r.returncode == 1 and "unknown argument" in r.stderr
+    r = run(["--query", "q", "--index", "i", "--pq_data", "p", "--data_type", "uint8", "--batched", "--entry", "x"])
+    assert r.returncode == 1 and "unrecognized entry" in r.stderr
+    r = run(["--query", "q", "--index", "i", "--pq_data", "p", "--data_type", "uint8", "--entry", "nearest"])
+    assert r.returncode == 1 and "applies to --batched only" in r.stderr
 
 
 @pytest.mark.gpu
@@ -75,5 +79,8 @@ def test_cli_recall_matches_oracle(golden, oracle_mod, tmp_path):
     for L, _, qps, rec in rows:
         assert float(qps) > 0 and abs(float(rec) - want[int(L)]) < 1e-6, (L, rec, want)
     r = run(base + ["--ef_search", "40", "-G", "--batched"])
+    assert r.returncode == 0, r.stderr
+    assert float(re.search(r"Recall @ 10: ([0-9.]+)", r.stdout).group(1)) > want[40] - 0.05
+    r = run(base + ["--ef_search", "40", "-G", "--batched", "--entry", "nearest"])
     assert r.returncode == 0, r.stderr
     assert float(re.search(r"Recall @ 10: ([0-9.]+)", r.stdout).group(1)) > want[40] - 0.05
