@@ -439,6 +439,10 @@ namespace {
 
 cudaError_t entry_scratch(gann_t* h, int nq);
 
+// Why a handle has no nearest-pivot operands (gann_open lays them out only for
+// a pivot graph whose tiles fit shared memory: 11 K slices of 16, dim <= 176).
+constexpr const char* kNoEntryPanel = "the nearest-pivot entry needs a pivot graph and dim <= 176";
+
 // Enqueue one batched search. counter / tables: caller-owned work counter and
 // BF16 table buffer (nq x M x 256) for concurrent launches; null = the handle's.
 int enqueue_batch(gann_t* h, const float* d_q, int nq, const int32_t* d_k, const int32_t* d_l, int k_max,
@@ -456,7 +460,7 @@ int enqueue_batch(gann_t* h, const float* d_q, int nq, const int32_t* d_k, const
   if (o.entry != GANN_ENTRY_NAV_WALK && o.entry != GANN_ENTRY_NEAREST_PIVOT)
     return set_error(GANN_EINVAL, "unknown entry");
   if (o.entry == GANN_ENTRY_NEAREST_PIVOT && !h->dx.entry_panel)
-    return set_error(GANN_ERANGE, "the nearest-pivot entry needs a pivot graph and dim <= 176");
+    return set_error(GANN_ERANGE, kNoEntryPanel);
   const int hb = o.hash_bits ? o.hash_bits : gann::batch_hash_bits(l_max) + h->tuned_hash_delta;
   if (hb < 4 || hb > 16) return set_error(GANN_EINVAL, "hash_bits must be in 4..16");
   const bool bf16 = prec != GANN_PREC_FP32;
@@ -573,7 +577,7 @@ int gann_nearest_pivots(gann_t* h, const float* d_queries, int nq, int32_t* d_pi
   if (nq < 0) return set_error(GANN_EINVAL, "nq must be >= 0");
   if (nq == 0) return GANN_OK;
   if (!d_queries) return set_error(GANN_EINVAL, "null buffer");
-  if (!h->dx.entry_panel) return set_error(GANN_ERANGE, "the nearest-pivot entry needs a pivot graph and dim <= 176");
+  if (!h->dx.entry_panel) return set_error(GANN_ERANGE, kNoEntryPanel);
   std::lock_guard<std::mutex> lk(h->mu);
   cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
   if (entry_scratch(h, nq) != cudaSuccess) return set_error(GANN_ENOMEM, "cannot allocate the entry keys");
