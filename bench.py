@@ -8,9 +8,12 @@ target (0.95). Prints one JSON line.
                     [--workload c2|c0|c1|c2_10m|small] [--forms plain,batched_bf16,...]
 
 The default workload is c2: 100M x 128 uint8 vectors (10,000-cluster mixture),
-Vamana-style graph R 32, PQ 32 x 256, a 1M-point pivot graph, all resident in
-HBM. The index is built once per box (about ten minutes, in a child process)
-and cached under --cache.
+graph R 32 (with the 1M-point sample's pivot graph embedded as long edges),
+PQ 32 x 256, a 100k-point pivot graph as the entry file, all resident in HBM.
+The index is built once per box (about four minutes, in a child process) and
+cached under --cache. The batched forms enter at each query's nearest pivot
+(--entry nearest, one tensor-core product per batch) unless --entry walk asks
+for the reference's pivot-graph walk; the plain form always takes the walk.
 
 Multi-GPU (torchrun, one process per GPU): every rank holds a replica of the
 index and searches its own full query batch (weak scaling, no collective on the
